@@ -1,0 +1,102 @@
+"""The oracle against fixtures produced by the reference's own C sources (tests/golden)."""
+import numpy as np
+import pytest
+
+import oracle
+
+
+def test_greedy_selection_matches_reference(golden):
+    g = golden
+    for c in range(len(g["g_n"])):
+        n, n2 = int(g["g_n"][c]), int(g["g_n2"][c])
+        a, b = g["g_off"][c], g["g_off"][c + 1]
+        w, P, Q = g["g_w"][a:b], g["g_p"][a:b], g["g_q"][a:b]
+        want = g["g_sel"][g["g_soff"][c]:g["g_soff"][c + 1]]
+        for ncp, nt in ((1, 1), (1, 4), (2, 1)):
+            got = oracle.select(n, w, P, Q, n2, id_ncp=ncp, nt=nt)
+            assert np.array_equal(got, want), (c, ncp, nt)
+
+
+def test_row_cyclic_pairs_match_reference(golden):
+    g = golden
+    off = 0
+    po = 0
+    for c in range(len(g["p_n"])):
+        n = int(g["p_n"][c])
+        J = g["p_j"][off:off + n]
+        nn = n * (n - 1) // 2
+        P, Q, tt = oracle.pairs(n, J, 2)
+        assert tt == g["p_nt"][c]
+        assert np.array_equal(P, g["p_p"][po:po + nn]) and np.array_equal(Q, g["p_q"][po:po + nn])
+        off += n
+        po += nn
+
+
+@pytest.mark.parametrize("kind", ["d", "z"])
+def test_2x2_hsvd_against_reference_80bit(golden, kind):
+    # sigma of the double-precision oracle within 1e-12 (relative) of the 80-bit reference kernel
+    B, J, S, I = golden[f"{kind}2_b"], golden[f"{kind}2_j"], golden[f"{kind}2_s"], golden[f"{kind}2_info"]
+    for k in range(len(B)):
+        A, U, Z, info = oracle.hsvd2(B[k], J[k], th1=1.0)
+        assert (info < 0) == (I[k] < 0)
+        if info < 0:
+            continue
+        s = np.array([A[0, 0].real, A[1, 1].real])
+        np.testing.assert_allclose(s, S[k], rtol=1e-12, atol=0)
+
+
+@pytest.mark.parametrize("kind", ["d", "z"])
+def test_2x2_dtest_residual(kind):
+    # the dtest/ztest recipe (src/D/dtest.F90:38-73): E = B - U^H diag(A) (J Z^H J), in extended precision
+    rng = np.random.Generator(np.random.PCG64(7))
+    worst = 0.0
+    for _ in range(500):
+        B = rng.standard_normal((2, 2)) * np.exp(rng.uniform(-8, 8, (2, 2)))
+        if kind == "z":
+            B = B + 1j * rng.standard_normal((2, 2))
+        J2 = [int(rng.choice([-1, 1])), int(rng.choice([-1, 1]))]
+        A, U, Z, info = oracle.hsvd2(B, J2, th1=1.0)
+        assert info >= 0
+        Jd = np.diag(np.array(J2, float))
+        lt = np.clongdouble if kind == "z" else np.longdouble
+        E = B.astype(lt) - U.conj().T.astype(lt) @ np.diag(np.diag(A)).astype(lt) @ (Jd @ Z.conj().T @ Jd).astype(lt)
+        worst = max(worst, float(np.max(np.abs(E)) / np.max(np.abs(B))))
+    assert worst < 1e-14
+
+
+def test_scale_exponent_hypot():
+    L = oracle.lib()
+    assert L.jo_exponent(1.0) == 1 and L.jo_exponent(0.5) == 0 and L.jo_exponent(5e-324) == -1073
+    assert L.jo_scale(5e-324, 1074) == 1.0
+    assert L.jo_scale(1.0, -1075) == 0.0 and L.jo_scale(1.5, -1074) == 5e-324 * 2  # ties to even
+    assert L.jo_scale(3.0, -1075) == 5e-324 * 2
+    rng = np.random.Generator(np.random.PCG64(3))
+    x = rng.standard_normal(2000) * np.exp(rng.uniform(-600, 600, 2000))
+    y = rng.standard_normal(2000) * np.exp(rng.uniform(-600, 600, 2000))
+    h = np.array([L.jo_hypot(a, b) for a, b in zip(x, y)])
+    ref = np.hypot(x.astype(np.longdouble), y.astype(np.longdouble))
+    assert np.max(np.abs(h - ref) / ref) < 1.2e-16
+
+
+def test_small_solve_invariants():
+    from jkogb_b200 import gen
+    for cplx in (False, True):
+        Y, J = (gen.complex_gaussian if cplx else gen.gaussian)(24, seed=11)
+        r = oracle.step_loop(Y, J, n_2=0, nt=2)
+        assert r["info"] > 0
+        U, Z, s = r["U"], r["Z"], r["sigma"]
+        assert np.linalg.norm(Y - U @ np.diag(s) @ Z) / np.linalg.norm(Y) < 1e-13
+        assert np.linalg.norm(U.conj().T @ U - np.eye(24)) < 1e-12
+        ev = np.sort(np.linalg.eigvalsh(Y @ np.diag(J.astype(float)) @ Y.conj().T))
+        assert np.max(np.abs(ev - np.sort(J * s * s))) / np.max(np.abs(ev)) < 1e-13
+
+
+def test_thread_count_determinism():
+    from jkogb_b200 import gen
+    Y, J = gen.gaussian(40, seed=5)
+    a = oracle.step_loop(Y, J, nt=1, trace=True)
+    b = oracle.step_loop(Y, J, nt=4, trace=True)
+    assert a["info"] == b["info"]
+    assert np.array_equal(a["trace"]["piv"], b["trace"]["piv"])
+    for k in ("U", "Z", "sigma"):
+        assert np.array_equal(a[k], b[k])
