@@ -1,0 +1,105 @@
+/*
+ * jkogb.h -- C ABI of libjkogb_b200.so: the J-Kogbetliantz hyperbolic SVD step loop
+ * of venovako/JKogb (real djk and complex zjk) on an NVIDIA B200 (sm_100a).
+ *
+ * The entry points replace the Fortran seam the reference's drivers call:
+ *   DSTEP_LOOP(N, U, LDU, A, LDA, Z, LDZ, J, SIGMA, NN, P, Q, R, NM, DZ, N_2, STEP, TT, W, INFO)
+ *     src/D/dstep.F90:472-604, called from src/D/djk.F90:253
+ *   ZSTEP_LOOP(...)  src/Z/zstep.F90:482-615, called from src/Z/zjk.F90
+ * together with the strategy plug-ins DPROC_INIT selects (src/D/dstep.F90:76-134):
+ * ID_NCP 0/1/2 (greedy non-colliding selection, AW_NCP1 == AW_NCP2) and ID_TRU 0/1/2
+ * (pair enumeration; the selection is a total order, so it does not change results).
+ * The caller's workspaces of the Fortran interface (NN, P, Q, NM, DZ, STEP, TT, W) live
+ * on the device and are not arguments here.
+ *
+ * Conventions: column-major matrices with a leading dimension; complex matrices are
+ * interleaved (re, im) doubles, the memory layout of Fortran COMPLEX(KIND=8); J holds
+ * the N signs (+1/-1) as int.  Return value INFO as DSTEP_LOOP's: >= 0 the number of
+ * steps with transformations, < 0 an error (see jk_strerror).  On return A holds the
+ * final matrix with a zeroed diagonal, SIGMA its diagonal (the hyperbolic singular
+ * values), U the accumulated left rotations and Z the inverse of the accumulated right
+ * transformation, J Z^T J (real) / J Z^H J (complex), so that Y = U diag(SIGMA) Z.
+ */
+#ifndef JKOGB_H
+#define JKOGB_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Options; a NULL pointer means all defaults (zero). */
+typedef struct {
+  int max_steps;    /* stop after this many steps (0: no limit); INFO = JK_ERR_MAX_STEPS when hit */
+  int zba_quirk;    /* complex BA branch of src/Z/ztransf.F90:325: 0 = as the reference (R1), 1 = R2 as the real code */
+  int graph_steps;  /* steps per CUDA-graph launch (0: 32; -1: plain stream launches) */
+  int device;       /* CUDA device ordinal for the host-pointer entry points (-1 or 0: current) */
+  int reserved[4];
+} jk_opts;
+
+/* Optional per-step trace, the stderr CSV of DSTEP_EXEC (src/D/dstep.F90:389-442) and
+ * the selected pivots of every step (the AW_OUT dump, src/shared/atypes.F90:30-77).
+ * Host buffers sized by the caller; unused pointers may be NULL. */
+typedef struct {
+  int max_steps;        /* capacity of sl/nl/trig/hyp/tw */
+  int *sl, *nl, *trig, *hyp;
+  double *tw;
+  long long max_piv;    /* capacity of piv in pivots */
+  int *piv;             /* 2 ints per pivot: p, q (1-based), in selection order, all steps */
+  long long n_piv;      /* out */
+  int n_steps;          /* out: steps recorded (including the last, empty one) */
+} jk_trace;
+
+#define JK_ERR_CUDA (-30)       /* a CUDA runtime error */
+#define JK_ERR_NOMEM (-31)      /* device allocation failed */
+#define JK_ERR_TOO_LARGE (-32)  /* N beyond this build's limit (see jk_max_order) */
+#define JK_ERR_ID_NCP (-21)     /* ID_NCP outside 0..2 */
+#define JK_ERR_ID_TRU (-22)     /* ID_TRU outside 0..2 */
+#define JK_ERR_J (-23)          /* a J entry is not +1 or -1 (TRU1/TRU2, src/shared/jstep.F90:38-39) */
+#define JK_ERR_MAX_STEPS (-24)  /* opts->max_steps reached */
+#define JK_ERR_NO_DEVICE (-33)  /* no CUDA device */
+
+/* DSTEP_LOOP with host buffers, src/D/dstep.F90:472-604 (copies to and from the device).
+ * A is in/out; U, Z, SIGMA are out.  N_2 is clamped as JSTEP_LEN does (src/shared/jstep.F90:124). */
+int jk_dstep_loop(int n, double *U, int ldu, double *A, int lda, double *Z, int ldz, const int *J,
+                  double *sigma, int n_2, int id_ncp, int id_tru, const jk_opts *opts, jk_trace *trace);
+
+/* ZSTEP_LOOP with host buffers, src/Z/zstep.F90:482-615; U, A, Z are complex (2 doubles each). */
+int jk_zstep_loop(int n, double *U, int ldu, double *A, int lda, double *Z, int ldz, const int *J,
+                  double *sigma, int n_2, int id_ncp, int id_tru, const jk_opts *opts, jk_trace *trace);
+
+/* The same loops on device buffers (leading dimension n), enqueued on `stream`
+ * (a cudaStream_t, NULL = the default stream); J is a host array.  Synchronises the
+ * stream before returning INFO. */
+int jk_dstep_loop_dev(int n, double *dU, double *dA, double *dZ, const int *J, double *dsigma,
+                      int n_2, int id_ncp, int id_tru, const jk_opts *opts, jk_trace *trace, void *stream);
+int jk_zstep_loop_dev(int n, double *dU, double *dA, double *dZ, const int *J, double *dsigma,
+                      int n_2, int id_ncp, int id_tru, const jk_opts *opts, jk_trace *trace, void *stream);
+
+/* A batch of independent 2x2 HSVDs on the device (DHSVD2 src/D/dtransf.F90:614,
+ * ZHSVD2 src/Z/ztransf.F90:925; the dtest/ztest kernel).  Host arrays: A, U, Z hold
+ * `count` column-major 2x2 blocks (4 reals or 4 complex each), J 2 signs per block;
+ * A is overwritten as DHSVD2 leaves it. */
+int jk_dhsvd2_batch(int count, double *A, const int *J, double *U, double *Z, int *info, double th1);
+int jk_zhsvd2_batch(int count, double *A, const int *J, double *U, double *Z, int *info, double th1);
+
+/* One build's pair weights (DMAGF2T/DMAGF2H, src/D/dstep.F90:189-219; ZMAGF2T/ZMAGF2H,
+ * src/Z/zstep.F90:191-221) on the device, returned as a symmetric n x n host matrix W
+ * (W[p + q*n] = weight of the pair (p, q), NaN where the reference stores a NaN). */
+int jk_dweights(int n, const double *A, int lda, const int *J, double *W);
+int jk_zweights(int n, const double *A, int lda, const int *J, double *W);
+
+/* The greedy non-colliding selection of one step (AW_SRT1/2 + AW_NCP1/2,
+ * src/shared/atypes.F90:85-484) on the device, from a symmetric n x n host weight
+ * matrix; writes SL pivots (1-based p < q) in selection order and returns SL. */
+int jk_select(int n, const double *W, int n_2, int *piv);
+
+/* Largest order N the loops accept. */
+int jk_max_order(int complex_);
+
+/* Text for an INFO code. */
+const char *jk_strerror(int info);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* !JKOGB_H */

@@ -1,0 +1,259 @@
+"""jkogb_b200: the J-Kogbetliantz hyperbolic SVD step loop of venovako/JKogb on a B200.
+
+Python host side of libjkogb_b200.so (C ABI in include/jkogb.h).  It mirrors the
+reference's interface for this path:
+
+  dstep_loop / zstep_loop   DSTEP_LOOP / ZSTEP_LOOP (src/D/dstep.F90:472, src/Z/zstep.F90:482)
+  step_loop                 either, chosen by the dtype of Y
+  step_loop_dev             the same on torch CUDA tensors, on the current stream
+  hsvd2_batch               DHSVD2 / ZHSVD2 on a batch of 2x2 blocks (src/D/dtransf.F90:614)
+  weights                   one build's pair weights (DMAGF2T/H, src/D/dstep.F90:12-72)
+  select                    the greedy non-colliding selection (AW_NCP1/2, src/shared/atypes.F90:359-484)
+  read_yj / write_uzs       the FN.Y / FN.J -> FN.YU / FN.ZZ / FN.SY file contract (src/D/bio.F90)
+
+All compute runs in the CUDA library; there is no CPU fallback.  Importing this
+module does not need a GPU, calling the compute entry points does.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+__all__ = ["lib", "step_loop", "dstep_loop", "zstep_loop", "step_loop_dev", "hsvd2_batch", "weights", "select",
+           "read_yj", "write_uzs", "JkError", "jstep_len", "SYMBOLS"]
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_lib", "libjkogb_b200.so")
+
+# every symbol include/jkogb.h declares
+SYMBOLS = ("jk_dstep_loop", "jk_zstep_loop", "jk_dstep_loop_dev", "jk_zstep_loop_dev", "jk_dhsvd2_batch",
+           "jk_zhsvd2_batch", "jk_dweights", "jk_zweights", "jk_select", "jk_max_order", "jk_strerror")
+
+
+class JkError(RuntimeError):
+    """A negative INFO from the library (or a missing library)."""
+
+    def __init__(self, info: int, what: str = ""):
+        self.info = info
+        super().__init__(f"{what}INFO={info}: {strerror(info) if _lib is not None else ''}")
+
+
+class Opts(C.Structure):
+    _fields_ = [("max_steps", C.c_int), ("zba_quirk", C.c_int), ("graph_steps", C.c_int), ("device", C.c_int),
+                ("reserved", C.c_int * 4)]
+
+
+class Trace(C.Structure):
+    _fields_ = [("max_steps", C.c_int), ("sl", C.POINTER(C.c_int)), ("nl", C.POINTER(C.c_int)),
+                ("trig", C.POINTER(C.c_int)), ("hyp", C.POINTER(C.c_int)), ("tw", C.POINTER(C.c_double)),
+                ("max_piv", C.c_longlong), ("piv", C.POINTER(C.c_int)), ("n_piv", C.c_longlong),
+                ("n_steps", C.c_int)]
+
+
+_lib = None
+
+
+def lib():
+    """Load libjkogb_b200.so (built in-tree by build()); raises if it is missing."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise JkError(-30, f"libjkogb_b200.so not built ({LIB_PATH}); run jkogb_b200.build.build(): ")
+        L = C.CDLL(LIB_PATH)
+        dp, ip, vp = C.POINTER(C.c_double), C.POINTER(C.c_int), C.c_void_p
+        for nm in ("jk_dstep_loop", "jk_zstep_loop"):
+            f = getattr(L, nm)
+            f.restype = C.c_int
+            f.argtypes = [C.c_int, vp, C.c_int, vp, C.c_int, vp, C.c_int, ip, vp, C.c_int, C.c_int, C.c_int,
+                          C.POINTER(Opts), C.POINTER(Trace)]
+        for nm in ("jk_dstep_loop_dev", "jk_zstep_loop_dev"):
+            f = getattr(L, nm)
+            f.restype = C.c_int
+            f.argtypes = [C.c_int, vp, vp, vp, ip, vp, C.c_int, C.c_int, C.c_int, C.POINTER(Opts), C.POINTER(Trace), vp]
+        for nm in ("jk_dhsvd2_batch", "jk_zhsvd2_batch"):
+            f = getattr(L, nm)
+            f.restype = C.c_int
+            f.argtypes = [C.c_int, vp, ip, vp, vp, ip, C.c_double]
+        for nm in ("jk_dweights", "jk_zweights"):
+            f = getattr(L, nm)
+            f.restype = C.c_int
+            f.argtypes = [C.c_int, vp, C.c_int, ip, dp]
+        L.jk_select.restype = C.c_int
+        L.jk_select.argtypes = [C.c_int, dp, C.c_int, ip]
+        L.jk_max_order.restype = C.c_int
+        L.jk_max_order.argtypes = [C.c_int]
+        L.jk_strerror.restype = C.c_char_p
+        L.jk_strerror.argtypes = [C.c_int]
+        _lib = L
+    return _lib
+
+
+def strerror(info: int) -> str:
+    return lib().jk_strerror(int(info)).decode()
+
+
+def jstep_len(n: int, n_2: int) -> int:
+    """JSTEP_LEN, src/shared/jstep.F90:124-133."""
+    if n_2 == 0:
+        return max(n // 2, 0)
+    return min(max(n_2, 0), n // 2)
+
+
+def _opts(max_steps=0, zba_quirk=0, graph_steps=0, device=0):
+    o = Opts()
+    o.max_steps, o.zba_quirk, o.graph_steps, o.device = int(max_steps), int(zba_quirk), int(graph_steps), int(device)
+    return o
+
+
+def _new_trace(max_steps, max_piv):
+    tr = Trace()
+    bufs = dict(sl=np.zeros(max_steps, np.int32), nl=np.zeros(max_steps, np.int32), trig=np.zeros(max_steps, np.int32),
+                hyp=np.zeros(max_steps, np.int32), tw=np.zeros(max_steps, np.float64),
+                piv=np.zeros(2 * max_piv, np.int32))
+    tr.max_steps, tr.max_piv = max_steps, max_piv
+    for k in ("sl", "nl", "trig", "hyp", "piv"):
+        setattr(tr, k, bufs[k].ctypes.data_as(C.POINTER(C.c_int)))
+    tr.tw = bufs["tw"].ctypes.data_as(C.POINTER(C.c_double))
+    return tr, bufs
+
+
+def _collect(tr, bufs):
+    m = min(tr.n_steps, len(bufs["sl"]))
+    return dict(n_steps=tr.n_steps, sl=bufs["sl"][:m].copy(), nl=bufs["nl"][:m].copy(), trig=bufs["trig"][:m].copy(),
+                hyp=bufs["hyp"][:m].copy(), tw=bufs["tw"][:m].copy(), piv=bufs["piv"][:2 * tr.n_piv].reshape(-1, 2).copy())
+
+
+def step_loop(Y, J, n_2=0, id_ncp=0, id_tru=0, trace=False, max_steps=0, zba_quirk=0, graph_steps=0,
+              trace_steps=1 << 16, trace_piv=1 << 22):
+    """DSTEP_LOOP / ZSTEP_LOOP on host arrays.  Y (n x n, float64 or complex128) is not modified.
+
+    Returns dict(info, A, U, Z, sigma[, trace]) with A the final matrix (diagonal zeroed),
+    U, Z such that Y = U diag(sigma) Z; raises JkError when INFO < 0.
+    """
+    Y = np.asarray(Y)
+    n = Y.shape[0]
+    cplx = np.iscomplexobj(Y)
+    dt = np.complex128 if cplx else np.float64
+    A = np.asfortranarray(Y.astype(dt, copy=True))
+    U = np.empty((n, n), dt, order="F")
+    Z = np.empty((n, n), dt, order="F")
+    s = np.empty(n, np.float64)
+    Jc = np.ascontiguousarray(np.asarray(J).astype(np.int32))
+    o = _opts(max_steps, zba_quirk, graph_steps)
+    trp, bufs = (_new_trace(trace_steps, trace_piv) if trace else (None, None))
+    f = lib().jk_zstep_loop if cplx else lib().jk_dstep_loop
+    info = f(n, U.ctypes.data, n, A.ctypes.data, n, Z.ctypes.data, n, Jc.ctypes.data_as(C.POINTER(C.c_int)),
+             s.ctypes.data, int(n_2), int(id_ncp), int(id_tru), C.byref(o), C.byref(trp) if trace else None)
+    if info < 0 and info != -24:
+        raise JkError(info, "step loop: ")
+    out = dict(info=info, A=A, U=U, Z=Z, sigma=s)
+    if trace:
+        out["trace"] = _collect(trp, bufs)
+    return out
+
+
+def dstep_loop(Y, J, n_2=0, id_ncp=0, id_tru=0, **kw):
+    return step_loop(np.asarray(Y, np.float64), J, n_2, id_ncp, id_tru, **kw)
+
+
+def zstep_loop(Y, J, n_2=0, id_ncp=0, id_tru=0, **kw):
+    return step_loop(np.asarray(Y, np.complex128), J, n_2, id_ncp, id_tru, **kw)
+
+
+def step_loop_dev(A, U, Z, sigma, J, n_2=0, id_ncp=0, id_tru=0, stream=None, max_steps=0, zba_quirk=0, graph_steps=0):
+    """The loop on torch CUDA tensors (n x n, column-major, i.e. the transpose of a
+    contiguous row-major tensor, float64 or complex128); J a host sequence.  A is
+    overwritten, U, Z, sigma are outputs.  Returns INFO; raises JkError when INFO < 0."""
+    import torch
+    n = A.shape[0]
+    cplx = A.dtype == torch.complex128
+    for t in (A, U, Z):
+        assert t.is_cuda and t.dtype == A.dtype and t.shape == (n, n)
+        assert t.stride() == (1, n), "column-major n x n tensors are expected (e.g. X.t() of a contiguous tensor)"
+    assert sigma.is_cuda and sigma.dtype == torch.float64 and sigma.numel() == n
+    Jc = np.ascontiguousarray(np.asarray(J).astype(np.int32))
+    o = _opts(max_steps, zba_quirk, graph_steps, A.device.index or 0)
+    st = stream if stream is not None else torch.cuda.current_stream(A.device)
+    f = lib().jk_zstep_loop_dev if cplx else lib().jk_dstep_loop_dev
+    info = f(n, U.data_ptr(), A.data_ptr(), Z.data_ptr(), Jc.ctypes.data_as(C.POINTER(C.c_int)), sigma.data_ptr(),
+             int(n_2), int(id_ncp), int(id_tru), C.byref(o), None, C.c_void_p(st.cuda_stream))
+    if info < 0 and info != -24:
+        raise JkError(info, "device step loop: ")
+    return info
+
+
+def hsvd2_batch(B, J, th1=0.75):
+    """A batch of 2x2 HSVDs (DHSVD2 / ZHSVD2) on the GPU.  B: (count, 2, 2), J: (count, 2).
+    Returns (A, U, Z, info) as DHSVD2 leaves them."""
+    B = np.asarray(B)
+    cplx = np.iscomplexobj(B)
+    dt = np.complex128 if cplx else np.float64
+    cnt = B.shape[0]
+    A = np.ascontiguousarray(np.transpose(B.astype(dt), (0, 2, 1)))  # column-major 2x2 blocks
+    U = np.empty_like(A)
+    Z = np.empty_like(A)
+    info = np.zeros(cnt, np.int32)
+    Jc = np.ascontiguousarray(np.asarray(J, np.int32))
+    f = lib().jk_zhsvd2_batch if cplx else lib().jk_dhsvd2_batch
+    rc = f(cnt, A.ctypes.data, Jc.ctypes.data_as(C.POINTER(C.c_int)), U.ctypes.data, Z.ctypes.data,
+           info.ctypes.data_as(C.POINTER(C.c_int)), float(th1))
+    if rc < 0:
+        raise JkError(rc, "hsvd2_batch: ")
+    tr = lambda X: np.transpose(X, (0, 2, 1))  # noqa: E731
+    return tr(A), tr(U), tr(Z), info
+
+
+def weights(A, J):
+    """Pair weights of one build on the GPU, as a symmetric n x n matrix (NaN = no transformation)."""
+    A = np.asarray(A)
+    n = A.shape[0]
+    cplx = np.iscomplexobj(A)
+    Af = np.asfortranarray(A.astype(np.complex128 if cplx else np.float64))
+    W = np.empty((n, n), np.float64, order="F")
+    Jc = np.ascontiguousarray(np.asarray(J, np.int32))
+    f = lib().jk_zweights if cplx else lib().jk_dweights
+    rc = f(n, Af.ctypes.data, n, Jc.ctypes.data_as(C.POINTER(C.c_int)), W.ctypes.data_as(C.POINTER(C.c_double)))
+    if rc < 0:
+        raise JkError(rc, "weights: ")
+    return W
+
+
+def select(W, n_2):
+    """The greedy non-colliding selection on the GPU from a symmetric n x n weight matrix;
+    returns the (SL, 2) pivots (1-based p < q) in selection order."""
+    W = np.asfortranarray(np.asarray(W, np.float64))
+    n = W.shape[0]
+    piv = np.zeros(2 * max(n // 2, 1), np.int32)
+    sl = lib().jk_select(n, W.ctypes.data_as(C.POINTER(C.c_double)), int(n_2), piv.ctypes.data_as(C.POINTER(C.c_int)))
+    if sl < 0:
+        raise JkError(sl, "select: ")
+    return piv[:2 * sl].reshape(-1, 2).copy()
+
+
+# ---- the file contract of djk / zjk (README.md:53-57; src/shared/binio.F90, src/D/bio.F90) ----
+
+def read_yj(fn: str, n: int, complex_: bool = False):
+    """Read FN.Y (n x n column-major float64 / complex128) and FN.J (n int64)."""
+    dt = np.complex128 if complex_ else np.float64
+    y = np.fromfile(fn + ".Y", dtype=dt, count=n * n)
+    if y.size != n * n:
+        raise JkError(1, f"{fn}.Y holds {y.size} of {n * n} entries: ")
+    j = np.fromfile(fn + ".J", dtype=np.int64, count=n)
+    if j.size != n:
+        raise JkError(2, f"{fn}.J holds {j.size} of {n} entries: ")
+    return y.reshape((n, n), order="F"), j
+
+
+def write_uzs(fn: str, U, Z, S):
+    """Write FN.YU, FN.ZZ (n x n column-major) and FN.SY (n float64)."""
+    np.asfortranarray(U).ravel(order="F").tofile(fn + ".YU")
+    np.asfortranarray(Z).ravel(order="F").tofile(fn + ".ZZ")
+    np.asarray(S, np.float64).tofile(fn + ".SY")
+
+
+def write_yj(fn: str, Y, J):
+    """Write FN.Y and FN.J (the inputs djk / zjk read)."""
+    np.asfortranarray(Y).ravel(order="F").tofile(fn + ".Y")
+    np.asarray(J, np.int64).tofile(fn + ".J")

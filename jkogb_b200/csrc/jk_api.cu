@@ -1,0 +1,392 @@
+// jk_api.cu -- the C ABI of libjkogb_b200.so (include/jkogb.h): device workspaces,
+// the step-loop driver (CUDA graphs of whole steps, a device-side stop flag read
+// back between graph launches) and the kernel-level entry points.
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+#include "../../include/jkogb.h"
+#include "jk_internal.h"
+
+using namespace jk;
+
+namespace {
+
+struct Guard {
+  std::vector<void *> dev;
+  void *pinned = nullptr;
+  ~Guard()
+  {
+    for (void *p : dev) cudaFree(p);
+    if (pinned) cudaFreeHost(pinned);
+  }
+  template <typename X> cudaError_t alloc(X **p, size_t bytes)
+  {
+    void *q = nullptr;
+    const cudaError_t e = cudaMalloc(&q, bytes ? bytes : 16);
+    if (e == cudaSuccess) { dev.push_back(q); *p = (X *)q; }
+    return e;
+  }
+};
+
+inline int cuda_fail(cudaError_t e)
+{
+  if (e == cudaErrorMemoryAllocation) { cudaGetLastError(); return JK_ERR_NOMEM; }
+  fprintf(stderr, "libjkogb_b200: CUDA error %d (%s)\n", (int)e, cudaGetErrorString(e));
+  cudaGetLastError();
+  return JK_ERR_CUDA;
+}
+
+#define CK(x) do { const cudaError_t e_ = (x); if (e_ != cudaSuccess) return cuda_fail(e_); } while (0)
+
+int max_order(int cplx)
+{
+  // k_rotate keeps two columns of A in shared memory and k_select its matching state
+  // (227 KB per block each); the tie key packs p in 16 bits
+  int n = (227 * 1024) / (2 * (cplx ? 16 : 8));
+  while (n > 3 && (select_smem(n) > 227 * 1024 || colsort_smem(n) > 227 * 1024)) --n;
+  return n < 65535 ? n : 65535;
+}
+
+// check the arguments as DSTEP_LOOP (src/D/dstep.F90:500-521) and DPROC_INIT / TRU do
+int check_args(int n, int ldu, int lda, int ldz, const int *J, int n_2, int id_ncp, int id_tru, int cplx)
+{
+  if (n < 3) return -1;
+  if (ldu < n) return -3;
+  if (lda < n) return -5;
+  if (ldz < n) return -7;
+  if (n_2 < 0) return -16;
+  if (id_ncp < 0 || id_ncp > 2) return JK_ERR_ID_NCP;
+  if (id_tru < 0 || id_tru > 2) return JK_ERR_ID_TRU;
+  if (!J) return -8;
+  for (int i = 0; i < n; ++i)
+    if (J[i] != 1 && J[i] != -1) return JK_ERR_J;
+  if (n > max_order(cplx)) return JK_ERR_TOO_LARGE;
+  return 0;
+}
+
+// JSTEP_LEN, src/shared/jstep.F90:124-133
+int jstep_len(int n, int n_2)
+{
+  if (!n_2) return (n / 2 > 0) ? n / 2 : 0;
+  const int a = (n_2 > 0) ? n_2 : 0;
+  return (a < n / 2) ? a : n / 2;
+}
+
+// device workspace of one solve
+int make_workspace(Guard &g, Workspace &w, int n, int cplx, const int *J, int trace_on, int cap_steps, long long cap_piv)
+{
+  memset(&w, 0, sizeof(w));
+  w.n = n;
+  w.cplx = cplx;
+  std::vector<int> plus, minus, j32(n);
+  for (int i = 0; i < n; ++i) {
+    j32[i] = J[i];
+    (J[i] == 1 ? plus : minus).push_back(i);
+  }
+  w.n_plus = (int)plus.size();
+  w.n_minus = (int)minus.size();
+  const size_t pivsz = cplx ? sizeof(Piv<double2>) : sizeof(Piv<double>);
+  const size_t rrsz = cplx ? sizeof(RowRot<double2>) : sizeof(RowRot<double>);
+  const int half = n / 2 + 1;
+  CK(g.alloc(&w.J, n * sizeof(int)));
+  CK(g.alloc(&w.plus, (plus.size() + 1) * sizeof(int)));
+  CK(g.alloc(&w.minus, (minus.size() + 1) * sizeof(int)));
+  CK(g.alloc(&w.Wm, (size_t)n * n * sizeof(double)));
+  CK(g.alloc(&w.piv, half * pivsz));
+  CK(g.alloc(&w.rowrot, half * rrsz));
+  CK(g.alloc(&w.list, (size_t)n * n * sizeof(unsigned short)));
+  CK(g.alloc(&w.rank, (size_t)n * n * sizeof(unsigned short)));
+  CK(g.alloc(&w.len, n * sizeof(int)));
+  CK(g.alloc(&w.ptr, n * sizeof(int)));
+  CK(g.alloc(&w.suitor, n * sizeof(unsigned)));
+  CK(g.alloc(&w.unp, (n + 1) * sizeof(int)));
+  CK(g.alloc(&w.st, sizeof(State)));
+  if (trace_on) {
+    const int cs = cap_steps > 0 ? cap_steps : 1;
+    const long long cp = cap_piv > 0 ? cap_piv : 1;
+    CK(g.alloc(&w.tr.sl, cs * sizeof(int)));
+    CK(g.alloc(&w.tr.nl, cs * sizeof(int)));
+    CK(g.alloc(&w.tr.trig, cs * sizeof(int)));
+    CK(g.alloc(&w.tr.hyp, cs * sizeof(int)));
+    CK(g.alloc(&w.tr.tw, cs * sizeof(double)));
+    CK(g.alloc(&w.tr.piv, cp * sizeof(int2)));
+  }
+  CK(cudaMallocHost((void **)&g.pinned, sizeof(State)));
+  w.st_host = (State *)g.pinned;
+  CK(cudaMemcpy(w.J, j32.data(), n * sizeof(int), cudaMemcpyHostToDevice));
+  if (!plus.empty()) CK(cudaMemcpy(w.plus, plus.data(), plus.size() * sizeof(int), cudaMemcpyHostToDevice));
+  if (!minus.empty()) CK(cudaMemcpy(w.minus, minus.data(), minus.size() * sizeof(int), cudaMemcpyHostToDevice));
+  State s0;
+  memset(&s0, 0, sizeof(s0));
+  s0.trace_on = trace_on;
+  s0.trace_cap_steps = trace_on ? cap_steps : 0;
+  s0.trace_cap_piv = trace_on ? cap_piv : 0;
+  CK(cudaMemcpy(w.st, &s0, sizeof(State), cudaMemcpyHostToDevice));
+  CK(prepare_kernels(n));
+  return 0;
+}
+
+// the loop of DSTEP_LOOP / ZSTEP_LOOP on device buffers
+int run_loop(int cplx, int n, void *dU, void *dA, void *dZ, const int *J, double *dsigma, int n_2, int id_ncp, int id_tru,
+             const jk_opts *opts, jk_trace *trace, cudaStream_t s)
+{
+  (void)id_ncp;
+  (void)id_tru;
+  jk_opts o;
+  memset(&o, 0, sizeof(o));
+  if (opts) o = *opts;
+  n_2 = jstep_len(n, n_2);
+  Guard g;
+  Workspace w;
+  const int trace_on = (trace != nullptr);
+  int rc = make_workspace(g, w, n, cplx, J, trace_on, trace ? trace->max_steps : 0, trace ? trace->max_piv : 0);
+  if (rc) return rc;
+  w.zba_quirk = (o.zba_quirk == 0) ? 1 : 0;
+
+  CK(launch_init(w, dU, dZ, s));
+  int chunk = (o.graph_steps == 0) ? 32 : o.graph_steps;
+  cudaGraphExec_t exec = nullptr;
+  if (chunk > 0) {
+    // capture `chunk` whole steps once; if capture fails, fall back to plain stream launches
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+      for (int k = 0; k < chunk && e == cudaSuccess; ++k) e = launch_step(w, dA, dU, dZ, n_2, s);
+      const cudaError_t e2 = cudaStreamEndCapture(s, &graph);
+      if (e == cudaSuccess) e = e2;
+    }
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
+    if (graph) cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      if (exec) { cudaGraphExecDestroy(exec); exec = nullptr; }
+      chunk = -1;
+    }
+  }
+  const int per_sync = (chunk > 0) ? chunk : 32;
+  // a bound on the number of steps (the loop has none of its own)
+  const long long cap = (o.max_steps > 0) ? o.max_steps : (4000LL * n + 100000LL);
+  long long launched = 0;
+  int info = 0;
+  for (;;) {
+    cudaError_t e = cudaSuccess;
+    if (exec) e = cudaGraphLaunch(exec, s);
+    else
+      for (int k = 0; k < per_sync && e == cudaSuccess; ++k) e = launch_step(w, dA, dU, dZ, n_2, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(w.st_host, w.st, sizeof(State), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
+      if (exec) cudaGraphExecDestroy(exec);
+      return cuda_fail(e);
+    }
+    launched += per_sync;
+    if (w.st_host->stop) { info = w.st_host->info; break; }
+    if (w.st_host->steps >= cap || launched > 2 * cap + per_sync) { info = JK_ERR_MAX_STEPS; break; }
+  }
+  if (exec) cudaGraphExecDestroy(exec);
+  CK(launch_finish(w, dA, dZ, dsigma, s));
+  if (trace) {
+    const State &h = *w.st_host;
+    const int ns = h.trace_steps < trace->max_steps ? h.trace_steps : trace->max_steps;
+    trace->n_steps = h.trace_steps;
+    if (ns > 0) {
+      if (trace->sl) CK(cudaMemcpyAsync(trace->sl, w.tr.sl, ns * sizeof(int), cudaMemcpyDeviceToHost, s));
+      if (trace->nl) CK(cudaMemcpyAsync(trace->nl, w.tr.nl, ns * sizeof(int), cudaMemcpyDeviceToHost, s));
+      if (trace->trig) CK(cudaMemcpyAsync(trace->trig, w.tr.trig, ns * sizeof(int), cudaMemcpyDeviceToHost, s));
+      if (trace->hyp) CK(cudaMemcpyAsync(trace->hyp, w.tr.hyp, ns * sizeof(int), cudaMemcpyDeviceToHost, s));
+      if (trace->tw) CK(cudaMemcpyAsync(trace->tw, w.tr.tw, ns * sizeof(double), cudaMemcpyDeviceToHost, s));
+    }
+    const long long np = h.trace_npiv < trace->max_piv ? h.trace_npiv : trace->max_piv;
+    trace->n_piv = np;
+    if (np > 0 && trace->piv) {
+      CK(cudaMemcpyAsync(trace->piv, w.tr.piv, np * sizeof(int2), cudaMemcpyDeviceToHost, s));
+      CK(cudaStreamSynchronize(s));
+      for (long long k = 0; k < 2 * np; ++k) trace->piv[k] += 1;
+    }
+  }
+  CK(cudaStreamSynchronize(s));
+  return info;
+}
+
+int pick_device(const jk_opts *opts)
+{
+  int cnt = 0;
+  if (cudaGetDeviceCount(&cnt) != cudaSuccess || cnt <= 0) { cudaGetLastError(); return JK_ERR_NO_DEVICE; }
+  if (opts && opts->device > 0) {
+    if (opts->device >= cnt) return JK_ERR_NO_DEVICE;
+    if (cudaSetDevice(opts->device) != cudaSuccess) return JK_ERR_CUDA;
+  }
+  return 0;
+}
+
+// host-buffer form: copy in (leading dimensions honoured), run, copy out
+int host_loop(int cplx, int n, double *U, int ldu, double *A, int lda, double *Z, int ldz, const int *J, double *sigma,
+              int n_2, int id_ncp, int id_tru, const jk_opts *opts, jk_trace *trace)
+{
+  int rc = check_args(n, ldu, lda, ldz, J, n_2, id_ncp, id_tru, cplx);
+  if (rc) return rc;
+  if ((rc = pick_device(opts))) return rc;
+  const size_t es = cplx ? 16 : 8;
+  Guard g;
+  void *dA, *dU, *dZ;
+  double *ds;
+  CK(g.alloc(&dA, (size_t)n * n * es));
+  CK(g.alloc(&dU, (size_t)n * n * es));
+  CK(g.alloc(&dZ, (size_t)n * n * es));
+  CK(g.alloc(&ds, n * sizeof(double)));
+  cudaStream_t s;
+  CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  CK(cudaMemcpy2DAsync(dA, n * es, A, (size_t)lda * es, n * es, n, cudaMemcpyHostToDevice, s));
+  const int info = run_loop(cplx, n, dU, dA, dZ, J, ds, n_2, id_ncp, id_tru, opts, trace, s);
+  if (info > JK_ERR_CUDA || info < JK_ERR_NO_DEVICE) {
+    CK(cudaMemcpy2DAsync(A, (size_t)lda * es, dA, n * es, n * es, n, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpy2DAsync(U, (size_t)ldu * es, dU, n * es, n * es, n, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpy2DAsync(Z, (size_t)ldz * es, dZ, n * es, n * es, n, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(sigma, ds, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+  }
+  CK(cudaStreamSynchronize(s));
+  cudaStreamDestroy(s);
+  return info;
+}
+
+}  // namespace
+
+extern "C" {
+
+int jk_dstep_loop(int n, double *U, int ldu, double *A, int lda, double *Z, int ldz, const int *J, double *sigma, int n_2,
+                  int id_ncp, int id_tru, const jk_opts *opts, jk_trace *trace)
+{
+  return host_loop(0, n, U, ldu, A, lda, Z, ldz, J, sigma, n_2, id_ncp, id_tru, opts, trace);
+}
+
+int jk_zstep_loop(int n, double *U, int ldu, double *A, int lda, double *Z, int ldz, const int *J, double *sigma, int n_2,
+                  int id_ncp, int id_tru, const jk_opts *opts, jk_trace *trace)
+{
+  return host_loop(1, n, U, ldu, A, lda, Z, ldz, J, sigma, n_2, id_ncp, id_tru, opts, trace);
+}
+
+int jk_dstep_loop_dev(int n, double *dU, double *dA, double *dZ, const int *J, double *dsigma, int n_2, int id_ncp, int id_tru,
+                      const jk_opts *opts, jk_trace *trace, void *stream)
+{
+  const int rc = check_args(n, n, n, n, J, n_2, id_ncp, id_tru, 0);
+  if (rc) return rc;
+  return run_loop(0, n, dU, dA, dZ, J, dsigma, n_2, id_ncp, id_tru, opts, trace, (cudaStream_t)stream);
+}
+
+int jk_zstep_loop_dev(int n, double *dU, double *dA, double *dZ, const int *J, double *dsigma, int n_2, int id_ncp, int id_tru,
+                      const jk_opts *opts, jk_trace *trace, void *stream)
+{
+  const int rc = check_args(n, n, n, n, J, n_2, id_ncp, id_tru, 1);
+  if (rc) return rc;
+  return run_loop(1, n, dU, dA, dZ, J, dsigma, n_2, id_ncp, id_tru, opts, trace, (cudaStream_t)stream);
+}
+
+static int hsvd2_batch(int cplx, int count, double *A, const int *J, double *U, double *Z, int *info, double th1)
+{
+  if (count < 0) return -1;
+  if (!count) return 0;
+  int rc = pick_device(nullptr);
+  if (rc) return rc;
+  const size_t bs = 4 * (cplx ? 16 : 8) * (size_t)count;
+  Guard g;
+  void *dA, *dU, *dZ;
+  int *dJ, *di;
+  CK(g.alloc(&dA, bs));
+  CK(g.alloc(&dU, bs));
+  CK(g.alloc(&dZ, bs));
+  CK(g.alloc(&dJ, 2 * sizeof(int) * (size_t)count));
+  CK(g.alloc(&di, sizeof(int) * (size_t)count));
+  CK(cudaMemcpy(dA, A, bs, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(dJ, J, 2 * sizeof(int) * (size_t)count, cudaMemcpyHostToDevice));
+  CK(launch_hsvd2_batch(cplx, count, dA, dJ, dU, dZ, di, th1, 0));
+  CK(cudaMemcpy(A, dA, bs, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(U, dU, bs, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(Z, dZ, bs, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(info, di, sizeof(int) * (size_t)count, cudaMemcpyDeviceToHost));
+  return 0;
+}
+
+int jk_dhsvd2_batch(int count, double *A, const int *J, double *U, double *Z, int *info, double th1)
+{
+  return hsvd2_batch(0, count, A, J, U, Z, info, th1);
+}
+
+int jk_zhsvd2_batch(int count, double *A, const int *J, double *U, double *Z, int *info, double th1)
+{
+  return hsvd2_batch(1, count, A, J, U, Z, info, th1);
+}
+
+static int weights(int cplx, int n, const double *A, int lda, const int *J, double *W)
+{
+  int rc = check_args(n, n, lda, n, J, 0, 0, 0, cplx);
+  if (rc) return rc;
+  if ((rc = pick_device(nullptr))) return rc;
+  const size_t es = cplx ? 16 : 8;
+  Guard g;
+  Workspace w;
+  rc = make_workspace(g, w, n, cplx, J, 0, 0, 0);
+  if (rc) return rc;
+  void *dA;
+  CK(g.alloc(&dA, (size_t)n * n * es));
+  CK(cudaMemcpy2D(dA, n * es, A, (size_t)lda * es, n * es, n, cudaMemcpyHostToDevice));
+  CK(cudaMemset(w.Wm, 0xFF, (size_t)n * n * sizeof(double)));  // all-ones bits: a NaN on the diagonal
+  CK(launch_weights(w, dA, 0));
+  CK(cudaMemcpy(W, w.Wm, (size_t)n * n * sizeof(double), cudaMemcpyDeviceToHost));
+  return 0;
+}
+
+int jk_dweights(int n, const double *A, int lda, const int *J, double *W) { return weights(0, n, A, lda, J, W); }
+int jk_zweights(int n, const double *A, int lda, const int *J, double *W) { return weights(1, n, A, lda, J, W); }
+
+int jk_select(int n, const double *W, int n_2, int *piv)
+{
+  if (n < 2) return -1;
+  if (n_2 < 0) return -16;
+  if (n > 65535) return JK_ERR_TOO_LARGE;
+  int rc = pick_device(nullptr);
+  if (rc) return rc;
+  n_2 = jstep_len(n, n_2);
+  std::vector<int> J(n, 1);
+  Guard g;
+  Workspace w;
+  rc = make_workspace(g, w, n, 0, J.data(), 0, 0, 0);
+  if (rc) return rc;
+  CK(cudaMemcpy(w.Wm, W, (size_t)n * n * sizeof(double), cudaMemcpyHostToDevice));
+  CK(launch_match(w, n_2, 0));
+  CK(cudaMemcpy(w.st_host, w.st, sizeof(State), cudaMemcpyDeviceToHost));
+  const int sl = w.st_host->sl;
+  std::vector<Piv<double>> pv(sl > 0 ? sl : 1);
+  if (sl > 0) CK(cudaMemcpy(pv.data(), w.piv, sl * sizeof(Piv<double>), cudaMemcpyDeviceToHost));
+  for (int i = 0; i < sl; ++i) { piv[2 * i] = pv[i].p + 1; piv[2 * i + 1] = pv[i].q + 1; }
+  return sl;
+}
+
+int jk_max_order(int complex_) { return max_order(complex_ ? 1 : 0); }
+
+const char *jk_strerror(int info)
+{
+  if (info >= 0) return "OK (number of steps)";
+  switch (info) {
+  case -1: return "N < 3";
+  case -3: return "LDU < N";
+  case -5: return "LDA < N";
+  case -7: return "LDZ < N";
+  case -8: return "J is NULL";
+  case -16: return "N_2 < 0";
+  case -10: return "a 2x2 hyperbolic transformation with |tanh| >= 1 (KHSVD2U)";
+  case -11: return "a 2x2 hyperbolic transformation with |tanh| >= 1 (KHSVD2L)";
+  case JK_ERR_ID_NCP: return "ID_NCP not in 0..2";
+  case JK_ERR_ID_TRU: return "ID_TRU not in 0..2";
+  case JK_ERR_J: return "a J entry is neither +1 nor -1";
+  case JK_ERR_MAX_STEPS: return "the step limit was reached";
+  case JK_ERR_CUDA: return "CUDA runtime error";
+  case JK_ERR_NOMEM: return "device memory allocation failed";
+  case JK_ERR_TOO_LARGE: return "N too large for this build";
+  case JK_ERR_NO_DEVICE: return "no CUDA device";
+  default: return "a 2x2 HSVD error (NaN or infinity in a pivot block) or argument error";
+  }
+}
+
+}  // extern "C"

@@ -1,0 +1,87 @@
+// jk_internal.h -- device data layout and host launch wrappers shared by the
+// CUDA translation units of libjkogb_b200 (not part of the public C ABI).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace jk {
+
+// Loop state kept on the device (one per solve).  Mirrors the scalars of
+// DSTEP_LOOP / DSTEP_EXEC (src/D/dstep.F90:376-604).
+struct State {
+  int stop;    // 1 once the loop has ended
+  int steps;   // S: steps with effective transformations
+  int info;    // final INFO (valid once stop)
+  int sl;      // SL of the current step (selected pivots)
+  int nl;      // NL: effective pivots of the current step
+  int err;     // minimum negative INFO over the current step's pivots (0 if none)
+  int nunp;    // columns outside the current pivot set
+  int rounds;  // matching rounds of the current step
+  int pending; // a step whose end-of-step test is still to run
+  int trace_on;
+  int trace_steps;      // steps recorded in the trace
+  int trace_cap_steps;  // capacity (steps) of the trace arrays
+  long long trace_npiv; // pivots recorded
+  long long trace_cap_piv;
+  double tw;   // sum of the weights of the effective pivots (NORMF2D column)
+  int trig, hyp;
+};
+
+// Per-step trace on the device (optional).
+struct Trace {
+  int *sl, *nl, *trig, *hyp;
+  double *tw;
+  int2 *piv;  // 0-based (p, q)
+};
+
+// One selected pivot (rank order) and its 2x2 transformation.
+template <typename T>
+struct Piv {
+  int p, q, info, pad;
+  double w;       // its weight (for the statistics)
+  T V[4];         // left 2x2 of DHSVD2 (before UT2/UH2)
+  T W[4];         // right 2x2 (Z of DHSVD2), W(:,1:2,I) of DSTEP_TRANSF
+  double d[2];    // W(1,3,I), W(2,3,I): the new diagonal
+};
+
+// Row-rotation record of one pivot: the BA coefficients of V (read by every block).
+template <typename T>
+struct RowRot {
+  int p, q, flags, pad;  // flags: bit0 c1, bit1 c2, bit2 apply
+  T r1, r2, m1, m2;
+};
+
+struct Workspace {
+  int n;
+  int cplx;
+  int n_plus, n_minus;
+  int *J;            // signs (device)
+  int *plus, *minus; // indices with J=+1 / J=-1, ascending
+  double *Wm;        // n x n pair weights, symmetric, NaN = no transformation
+  void *piv;         // Piv<T>[n/2]
+  void *rowrot;      // RowRot<T>[n/2]
+  unsigned short *list;  // n x n: the partners of every vertex, best first
+  unsigned short *rank;  // n x n: rank[v][u] = position of u in v's list
+  int *len;              // valid entries of each list
+  int *ptr;              // resume position of each vertex's proposals
+  unsigned *suitor;      // (rank << 16 | vertex) of each vertex's current suitor
+  int *unp;              // columns outside the current pivot set
+  State *st;         // device state
+  State *st_host;    // pinned host mirror
+  Trace tr;
+  int zba_quirk;
+};
+
+// host launchers (jk_kernels.cu)
+cudaError_t launch_init(Workspace &w, void *U, void *Z, cudaStream_t s);
+cudaError_t launch_step(Workspace &w, void *A, void *U, void *Z, int n_2, cudaStream_t s);
+cudaError_t launch_finish(Workspace &w, void *A, void *Z, double *sigma, cudaStream_t s);
+cudaError_t launch_weights(Workspace &w, const void *A, cudaStream_t s);
+cudaError_t launch_match(Workspace &w, int n_2, cudaStream_t s);
+cudaError_t launch_hsvd2_batch(int cplx, int count, void *A, const int *J, void *U, void *Z, int *info, double th1, cudaStream_t s);
+cudaError_t prepare_kernels(int n);
+size_t select_smem(int n);
+size_t colsort_smem(int n);
+
+}  // namespace jk

@@ -1,0 +1,906 @@
+// jk_kernels.cu -- the per-step CUDA kernels of the J-Kogbetliantz HSVD (real and
+// complex), B200 (sm_100a).  One step of DSTEP_EXEC / ZSTEP_EXEC
+// (src/D/dstep.F90:376-443, src/Z/zstep.F90:379-447) is six launches:
+//
+//   k_weights_trig  pair weights of the trigonometric pairs      (DMAGF2T / ZMAGF2T)
+//   k_weights_hyp   pair weights of the hyperbolic pairs         (DMAGF2H / ZMAGF2H)
+//                   = batched 2x2 HSVD + the tiled off-norm scan (ABODNDF2 / ABODNZF2)
+//   k_colsort       every vertex's partners ranked by the records' sort order (AW_CMP)
+//   k_suitor        the greedy non-colliding selection (AW_SRT* + AW_NCP1/2) as the
+//                   greedy matching, by lock-free suitor proposals
+//   k_select        one block: the end-of-step test of the previous step
+//                   (SL := MIN(SL, NL)), the ranking of the matched pairs, the first
+//                   N_2 of them, and the 2x2 HSVD of every selected pivot
+//                   (DHSVD2 / ZHSVD2) with INFO and NL
+//   k_rotate        fused transformations: every block loads a column pair of A,
+//                   applies all row rotations (BA), then its column rotation (AB)
+//                   and the diagonal write-back, and rotates the columns of U and Z
+//
+// Matrices are column-major with leading dimension n; complex entries are double2.
+#include <cooperative_groups.h>
+
+#include "jk_internal.h"
+#include "jk_math.cuh"
+#include "jk_zmath.cuh"
+
+namespace cg = cooperative_groups;
+
+namespace jk {
+
+// ---------------------------------------------------------------------------
+// scalar traits: the real (double) and complex (double2) flavours
+// ---------------------------------------------------------------------------
+template <typename T> struct Tr;
+
+template <> struct Tr<double> {
+  typedef Rot R;
+  static __device__ __forceinline__ double zero() { return 0.0; }
+  static __device__ __forceinline__ double one() { return 1.0; }
+  static __device__ __forceinline__ double re(double a) { return a; }
+  static __device__ __forceinline__ bool nonzero(double a) { return a != 0.0; }
+  static __device__ __forceinline__ bool imnz(double) { return false; }
+  static __device__ __forceinline__ double conj_(double a) { return a; }
+  static __device__ __forceinline__ double neg_(double a) { return -a; }
+  static __device__ __forceinline__ double magt(double aqp, double apq) { return dasum2(aqp, apq); }
+  static __device__ __forceinline__ void hsvd2(double A[4], int j0, int j1, double U[4], double Z[4], double th1, int &info) { dhsvd2(A, j0, j1, U, Z, th1, info); }
+  static __device__ __forceinline__ R ba(const double B[4], int) { return rot_ba(B); }
+  static __device__ __forceinline__ R ab(const double B[4]) { return rot_ab(B); }
+  static __device__ __forceinline__ void apply_ba(const R &t, double &x, double &y) { rot_apply(t, x, y); }
+  static __device__ __forceinline__ void apply_ab(const R &t, double &x, double &y) { rot_apply(t, x, y); }
+  // UT2, src/D/dtransf.F90:42-51
+  static __device__ __forceinline__ void ut2(double V[4]) { const double t = V[M21]; V[M21] = V[M12]; V[M12] = t; }
+};
+
+template <> struct Tr<double2> {
+  typedef ZRot R;
+  static __device__ __forceinline__ double2 zero() { return make_double2(0.0, 0.0); }
+  static __device__ __forceinline__ double2 one() { return make_double2(1.0, 0.0); }
+  static __device__ __forceinline__ double re(double2 a) { return a.x; }
+  static __device__ __forceinline__ bool nonzero(double2 a) { return !zeq0(a); }
+  static __device__ __forceinline__ bool imnz(double2 a) { return a.y != 0.0; }
+  static __device__ __forceinline__ double2 conj_(double2 a) { return conj(a); }
+  static __device__ __forceinline__ double2 neg_(double2 a) { return zneg(a); }
+  static __device__ __forceinline__ double magt(double2 aqp, double2 apq) { return dasum4(aqp.x, aqp.y, apq.x, apq.y); }
+  static __device__ __forceinline__ void hsvd2(double2 A[4], int j0, int j1, double2 U[4], double2 Z[4], double th1, int &info) { zhsvd2(A, j0, j1, U, Z, th1, info); }
+  static __device__ __forceinline__ R ba(const double2 B[4], int quirk) { return zrot_ba(B, quirk); }
+  static __device__ __forceinline__ R ab(const double2 B[4]) { return zrot_ab(B); }
+  static __device__ __forceinline__ void apply_ba(const R &t, double2 &x, double2 &y) { zrot_apply_ba(t, x, y); }
+  static __device__ __forceinline__ void apply_ab(const R &t, double2 &x, double2 &y) { zrot_apply_ab(t, x, y); }
+  // UH2, src/Z/ztransf.F90:79-90
+  static __device__ __forceinline__ void ut2(double2 V[4])
+  {
+    V[M11] = conj(V[M11]);
+    const double2 u21 = V[M21];
+    V[M21] = conj(V[M12]);
+    V[M12] = conj(u21);
+    V[M22] = conj(V[M22]);
+  }
+};
+
+__device__ __forceinline__ double nan_w() { return __longlong_as_double(0x7FF8000000000000LL); }
+
+// "a transformation may be needed" of DMAGF2T/DMAGF2H (src/D/dstep.F90:19-20, 49-50)
+// and ZMAGF2T/ZMAGF2H (src/Z/zstep.F90:19-21, 51-52)
+template <typename T>
+__device__ __forceinline__ bool may_transform(T app, T aqp, T apq, T aqq)
+{
+  return Tr<T>::nonzero(aqp) || Tr<T>::nonzero(apq) || Tr<T>::imnz(app) || Tr<T>::imnz(aqq) ||
+         neg(Tr<T>::re(app)) || neg(Tr<T>::re(aqq));
+}
+
+// ---------------------------------------------------------------------------
+// initialisation and finalisation
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void k_identity2(T *U, T *Z, int n)
+{
+  const long long nn = (long long)n * n;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < nn; k += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(k % n), j = (int)(k / n);
+    const T v = (i == j) ? Tr<T>::one() : Tr<T>::zero();
+    U[k] = v;
+    Z[k] = v;
+  }
+}
+
+__global__ void k_state_init(State *st)
+{
+  const int cap_s = st->trace_cap_steps, on = st->trace_on;
+  const long long cap_p = st->trace_cap_piv;
+  State z = {};
+  z.trace_on = on;
+  z.trace_cap_steps = cap_s;
+  z.trace_cap_piv = cap_p;
+  z.tw = -0.0;
+  *st = z;
+}
+
+// SIGMA(S) = A(S,S); A(S,S) = 0   (src/D/dstep.F90:594-602, src/Z/zstep.F90:605-613)
+template <typename T>
+__global__ void k_sigma(T *A, double *sigma, int n)
+{
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const long long k = (long long)i * n + i;
+    sigma[i] = Tr<T>::re(A[k]);
+    A[k] = Tr<T>::zero();
+  }
+}
+
+// Z := J Z^T J (JZTJ, src/D/dstep.F90:447-468) or J Z^H J (JZHJ, src/Z/zstep.F90:451-478),
+// in place, one 32x32 tile pair per block
+template <typename T>
+__global__ void k_jztj(T *Z, const int *J, int n)
+{
+  __shared__ T a[32][33], b[32][33];
+  const int nt = (n + 31) / 32;
+  // block -> (ti, tj), ti <= tj
+  int t = blockIdx.x, ti = 0;
+  while (t >= nt - ti) { t -= nt - ti; ++ti; }
+  const int tj = ti + t;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  for (int r = ty; r < 32; r += blockDim.y) {
+    const int i1 = ti * 32 + tx, j1 = tj * 32 + r;  // tile (ti, tj): rows ti, cols tj
+    const int i2 = tj * 32 + tx, j2 = ti * 32 + r;  // tile (tj, ti)
+    if (i1 < n && j1 < n) a[r][tx] = Z[(long long)j1 * n + i1];
+    if (i2 < n && j2 < n) b[r][tx] = Z[(long long)j2 * n + i2];
+  }
+  __syncthreads();
+  for (int r = ty; r < 32; r += blockDim.y) {
+    // new Z(i, j) = J_i conj(Z(j, i)) J_j
+    const int i1 = ti * 32 + tx, j1 = tj * 32 + r;
+    if (i1 < n && j1 < n && (ti != tj || i1 <= j1)) {
+      T v = Tr<T>::conj_(b[tx][r]);            // old Z(j1, i1)
+      if (i1 != j1 && J[i1] != J[j1]) v = Tr<T>::neg_(v);
+      if (ti == tj && i1 == j1) v = Tr<T>::conj_(a[r][tx]);
+      Z[(long long)j1 * n + i1] = v;
+    }
+    const int i2 = tj * 32 + tx, j2 = ti * 32 + r;
+    if (ti != tj && i2 < n && j2 < n) {
+      T v = Tr<T>::conj_(a[tx][r]);            // old Z(j2, i2)
+      if (J[i2] != J[j2]) v = Tr<T>::neg_(v);
+      Z[(long long)j2 * n + i2] = v;
+    }
+  }
+  if (ti == tj) {
+    // the lower half of a diagonal tile
+    __syncthreads();
+    for (int r = ty; r < 32; r += blockDim.y) {
+      const int i1 = ti * 32 + tx, j1 = tj * 32 + r;
+      if (i1 < n && j1 < n && i1 > j1) {
+        T v = Tr<T>::conj_(a[tx][r]);
+        if (J[i1] != J[j1]) v = Tr<T>::neg_(v);
+        Z[(long long)j1 * n + i1] = v;
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// weights of the trigonometric pairs: DMAGF2T (src/D/dstep.F90:12-37),
+// ZMAGF2T (src/Z/zstep.F90:12-39); one thread per (p, q), both halves of Wm written
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void k_weights_trig(const State *st, const T *__restrict__ A, const int *__restrict__ J, double *__restrict__ Wm, int n)
+{
+  if (st->stop) return;
+  const int p = blockIdx.x * 32 + threadIdx.x, q = blockIdx.y * 8 + threadIdx.y;
+  if (p >= n || q >= n || p >= q) return;
+  const int s = J[p] + J[q];
+  if (s != 2 && s != -2) return;  // hyperbolic pairs are the other kernel's
+  const T app = A[(long long)p * n + p], aqp = A[(long long)p * n + q], apq = A[(long long)q * n + p], aqq = A[(long long)q * n + q];
+  const bool nz = may_transform(app, aqp, apq, aqq);
+  double w;
+  if (s == -2) w = (nz || (Tr<T>::re(aqq) < Tr<T>::re(app))) ? Tr<T>::magt(aqp, apq) : nan_w();
+  else w = (nz || (Tr<T>::re(app) < Tr<T>::re(aqq))) ? Tr<T>::magt(aqp, apq) : nan_w();
+  Wm[(long long)q * n + p] = w;
+  Wm[(long long)p * n + q] = w;
+}
+
+// ---------------------------------------------------------------------------
+// weights of the hyperbolic pairs: DMAGF2H (src/D/dstep.F90:41-72) with ABODNDF2
+// (src/D/dtransf.F90:246-348), ZMAGF2H (src/Z/zstep.F90:43-74) with ABODNZF2
+// (src/Z/ztransf.F90:452-637).  A block owns HP "+" columns x HM "-" columns; each
+// thread owns one pair and keeps the reference's sequential row order in its own
+// fma chain, while the column data are staged through shared memory in row chunks
+// and reused by the whole tile.  The -inf of a weight becomes NaN (src/D/dstep.F90:212-214).
+// ---------------------------------------------------------------------------
+#define HR 64
+
+__device__ __forceinline__ void scan_rows_real(const double *xs, const double *ys, int rows, int i0, int p, int q, const Rot &t, double &d)
+{
+  if (t.c1 && t.c2) {
+#pragma unroll 4
+    for (int r = 0; r < rows; ++r) {
+      const double x = xs[r], y = ys[r];
+      const double xx = __dmul_rn(fma(y, t.r1, x), t.m1);
+      const double yy = __dmul_rn(fma(x, t.r2, y), t.m2);
+      const int i = i0 + r;
+      if (i != p && i != q) {
+        d = fma(__dsub_rn(x, xx), __dadd_rn(x, xx), d);
+        d = fma(__dsub_rn(y, yy), __dadd_rn(y, yy), d);
+      }
+    }
+  }
+  else {
+    for (int r = 0; r < rows; ++r) {
+      double x = xs[r], y = ys[r];
+      const double x0 = x, y0 = y;
+      rot_apply(t, x, y);
+      const int i = i0 + r;
+      if (i != p && i != q) {
+        d = fma(__dsub_rn(x0, x), __dadd_rn(x0, x), d);
+        d = fma(__dsub_rn(y0, y), __dadd_rn(y0, y), d);
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ void scan_rows_cplx(const double2 *xs, const double2 *ys, int rows, int i0, int p, int q, const ZRot &t, double &d)
+{
+  for (int r = 0; r < rows; ++r) {
+    double2 x = xs[r], y = ys[r];
+    const double2 x0 = x, y0 = y;
+    zrot_apply_ab(t, x, y);
+    const int i = i0 + r;
+    if (i != p && i != q) {
+      const double axi = zabs(x0), axx = zabs(x), ayi = zabs(y0), ayy = zabs(y);
+      d = fma(__dsub_rn(axi, axx), __dadd_rn(axi, axx), d);
+      d = fma(__dsub_rn(ayi, ayy), __dadd_rn(ayi, ayy), d);
+    }
+  }
+}
+
+template <typename T, int HP, int HM>
+__global__ void __launch_bounds__(HP * HM)
+k_weights_hyp(const State *st, const T *__restrict__ A, const int *__restrict__ plus, const int *__restrict__ minus,
+              int n_plus, int n_minus, double *__restrict__ Wm, int n)
+{
+  if (st->stop) return;
+  __shared__ T sP[HP][HR + 1];
+  __shared__ T sM[HM][HR + 1];
+  const int tx = threadIdx.x % HP, ty = threadIdx.x / HP;
+  const int ia = blockIdx.x * HP + tx, ib = blockIdx.y * HM + ty;
+  const bool valid = (ia < n_plus) && (ib < n_minus);
+  int p = 0, q = 0;
+  bool scan = false, a_is_p = true;
+  double d = 0.0, w = nan_w();
+  typename Tr<T>::R t;
+  if (valid) {
+    const int a = plus[ia], b = minus[ib];
+    a_is_p = (a < b);
+    p = a_is_p ? a : b;
+    q = a_is_p ? b : a;
+    const T app = A[(long long)p * n + p], aqp = A[(long long)p * n + q], apq = A[(long long)q * n + p], aqq = A[(long long)q * n + q];
+    if (may_transform(app, aqp, apq, aqq)) {
+      T A2[4] = { app, aqp, apq, aqq }, U2[4], Z2[4];
+      int info = 0;
+      const int jp = a_is_p ? 1 : -1;  // "+" column a, "-" column b
+      Tr<T>::hsvd2(A2, jp, -jp, U2, Z2, JK_TH1FIX, info);
+      if (info < 0) w = nan_w();
+      else if (!(info & 1)) w = 0.0;
+      else if (!(info & 4)) w = Tr<T>::magt(aqp, apq);
+      else {
+        // the two off-diagonal terms that start ABODNDF2 / ABODNZF2
+        const T aqp2 = (info & 8) ? A2[M21] : Tr<T>::zero();
+        const T apq2 = (info & 8) ? A2[M12] : Tr<T>::zero();
+        if constexpr (sizeof(T) == sizeof(double)) {
+          const double xq = *(const double *)&aqp, yp = *(const double *)&apq;
+          const double a1 = *(const double *)&aqp2, a2 = *(const double *)&apq2;
+          d = 0.0;
+          d = fma(__dsub_rn(xq, a1), __dadd_rn(xq, a1), d);
+          d = fma(__dsub_rn(yp, a2), __dadd_rn(yp, a2), d);
+        }
+        else {
+          const double2 xq = *(const double2 *)&aqp, yp = *(const double2 *)&apq;
+          const double2 a1 = *(const double2 *)&aqp2, a2 = *(const double2 *)&apq2;
+          d = 0.0;
+          d = fma(__dsub_rn(xq.x, a1.x), __dadd_rn(xq.x, a1.x), d);
+          d = fma(__dsub_rn(xq.y, a1.y), __dadd_rn(xq.y, a1.y), d);
+          d = fma(__dsub_rn(yp.x, a2.x), __dadd_rn(yp.x, a2.x), d);
+          d = fma(__dsub_rn(yp.y, a2.y), __dadd_rn(yp.y, a2.y), d);
+        }
+        t = Tr<T>::ab(Z2);
+        scan = true;
+      }
+    }
+  }
+  // a block-uniform exit when no thread of the tile scans
+  if (!__syncthreads_or(scan)) {
+    if (valid) {
+      if (w < -JK_HUGE) w = nan_w();
+      Wm[(long long)q * n + p] = w;
+      Wm[(long long)p * n + q] = w;
+    }
+    return;
+  }
+  const int pa = blockIdx.x * HP, pb = blockIdx.y * HM;
+  for (int i0 = 0; i0 < n; i0 += HR) {
+    const int rows = min(HR, n - i0);
+    // stage rows [i0, i0+rows) of the tile's HP + HM columns
+    for (int k = threadIdx.x; k < (HP + HM) * HR; k += HP * HM) {
+      const int c = k / HR, r = k % HR;
+      if (r < rows) {
+        if (c < HP) {
+          const int ca = pa + c;
+          if (ca < n_plus) sP[c][r] = A[(long long)plus[ca] * n + i0 + r];
+        }
+        else {
+          const int cb = pb + (c - HP);
+          if (cb < n_minus) sM[c - HP][r] = A[(long long)minus[cb] * n + i0 + r];
+        }
+      }
+    }
+    __syncthreads();
+    if (scan) {
+      const T *xs = a_is_p ? sP[tx] : sM[ty];
+      const T *ys = a_is_p ? sM[ty] : sP[tx];
+      if constexpr (sizeof(T) == sizeof(double)) scan_rows_real((const double *)xs, (const double *)ys, rows, i0, p, q, *(const Rot *)&t, d);
+      else scan_rows_cplx((const double2 *)xs, (const double2 *)ys, rows, i0, p, q, *(const ZRot *)&t, d);
+    }
+    __syncthreads();
+  }
+  if (valid) {
+    if (scan) w = d;
+    if (w < -JK_HUGE) w = nan_w();
+    Wm[(long long)q * n + p] = w;
+    Wm[(long long)p * n + q] = w;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// selection: the greedy non-colliding pivots of the sorted record list
+// (AW_SRT1/2 + AW_NCP1/2, src/shared/atypes.F90:85-484)
+//
+// The records are ordered by descending weight, then descending band q-p, then
+// descending p (AW_CMP).  Walking them in that order and taking every record whose
+// p and q are both unused is the greedy matching of the weighted graph.  The walk
+// stops after N_2 records: those are the N_2 highest-ranked edges of the full
+// greedy matching, so the matched edges are ranked and the first N_2 kept, in rank
+// order (the STEP array).
+//
+// The matching is computed with the Suitor algorithm (Manne and Halappanavar,
+// IPDPS 2014), which yields exactly the greedy matching for a total order of the
+// edges: every vertex proposes to its best partner for which it beats that
+// partner's current suitor; a displaced suitor proposes again further down its
+// list.  k_colsort ranks every vertex's partners (one block per column of the
+// symmetric weight matrix, a bitonic sort in shared memory); k_suitor runs the
+// proposals, one thread per vertex, with atomicCAS on a (rank << 16 | suitor) word
+// per vertex and no barriers; k_select collects the mutual pairs.
+// ---------------------------------------------------------------------------
+#define SEL_THREADS 512
+#define SORT_THREADS 512
+#define SUITOR_EMPTY 0xFFFFFFFFu
+
+// order-preserving 64-bit key of a weight; 0 for NaN (no record); -0 == +0
+__device__ __forceinline__ unsigned long long wkey(double w)
+{
+  if (w != w) return 0ULL;
+  const unsigned long long b = (unsigned long long)__double_as_longlong((w == 0.0) ? 0.0 : w);
+  return (b >> 63) ? ~b : (b | 0x8000000000000000ULL);
+}
+
+// the tie key: larger band first, then larger p (0-based indices, n <= 65535)
+__device__ __forceinline__ unsigned tkey(int u, int v)
+{
+  const int p = (u < v) ? u : v, b = (u < v) ? (v - u) : (u - v);
+  return ((unsigned)b << 16) | (unsigned)p;
+}
+
+__device__ __forceinline__ bool kbetter(unsigned long long k1, unsigned t1, unsigned long long k2, unsigned t2)
+{
+  return (k1 > k2) || ((k1 == k2) && (t1 > t2));
+}
+
+// descending bitonic sort of s2 (a power of two) records (k, t, i) in shared memory
+__device__ __forceinline__ void bitonic_desc(unsigned long long *k, unsigned *t, int *ix, int s2)
+{
+  for (int kk = 2; kk <= s2; kk <<= 1)
+    for (int j = kk >> 1; j > 0; j >>= 1) {
+      for (int i = threadIdx.x; i < s2; i += blockDim.x) {
+        const int l = i ^ j;
+        if (l > i) {
+          const bool desc = ((i & kk) == 0);
+          const bool lbetter = kbetter(k[l], t[l], k[i], t[i]);
+          if (desc == lbetter) {
+            const unsigned long long a = k[i]; k[i] = k[l]; k[l] = a;
+            const unsigned b = t[i]; t[i] = t[l]; t[l] = b;
+            const int c = ix[i]; ix[i] = ix[l]; ix[l] = c;
+          }
+        }
+      }
+      __syncthreads();
+    }
+}
+
+__host__ __device__ __forceinline__ int pow2ceil(int x)
+{
+  int s = 1;
+  while (s < x) s <<= 1;
+  return s;
+}
+
+// rank the partners of vertex x = blockIdx.x: list[x][r] = r-th best partner,
+// rank[x][u] = position of u in that list; also resets the vertex's suitor state
+__global__ void __launch_bounds__(SORT_THREADS)
+k_colsort(const State *st, const double *__restrict__ Wm, int n, unsigned short *list, unsigned short *rank, int *len,
+          int *ptr, unsigned *suitor)
+{
+  if (st->stop) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int s2 = pow2ceil(n);
+  unsigned long long *k = (unsigned long long *)smem_raw;
+  unsigned *t = (unsigned *)(k + s2);
+  int *ix = (int *)(t + s2);
+  const int x = blockIdx.x;
+  const double *col = Wm + (long long)x * n;
+  __shared__ int s_cnt;
+  if (threadIdx.x == 0) s_cnt = 0;
+  __syncthreads();
+  int valid = 0;
+  for (int u = threadIdx.x; u < s2; u += blockDim.x) {
+    unsigned long long kk = 0ULL;
+    if (u < n && u != x) kk = wkey(col[u]);
+    k[u] = kk;
+    t[u] = kk ? tkey(u, x) : 0u;
+    ix[u] = kk ? u : -1;
+    valid += kk ? 1 : 0;
+  }
+  atomicAdd(&s_cnt, valid);
+  __syncthreads();
+  const int cnt = s_cnt;
+  bitonic_desc(k, t, ix, s2);
+  unsigned short *lx = list + (long long)x * n;
+  unsigned short *rx = rank + (long long)x * n;
+  for (int r = threadIdx.x; r < cnt; r += blockDim.x) {
+    const int u = ix[r];
+    lx[r] = (unsigned short)u;
+    rx[u] = (unsigned short)r;
+  }
+  if (threadIdx.x == 0) {
+    len[x] = cnt;
+    ptr[x] = 0;
+    suitor[x] = SUITOR_EMPTY;
+  }
+}
+
+// the proposals: one thread per vertex; a thread that displaces a suitor continues
+// with the displaced vertex.  Every proposal either moves a list pointer forward or
+// strictly improves a suitor's rank, so the work is bounded (guard: 4 n^2 steps).
+#define SUITOR_BATCH 4
+__global__ void __launch_bounds__(128)
+k_suitor(State *st, int n, const unsigned short *__restrict__ list, const unsigned short *__restrict__ rank,
+         const int *__restrict__ len, int *ptr, unsigned *suitor)
+{
+  if (st->stop) return;
+  int cur = blockIdx.x * blockDim.x + threadIdx.x;
+  if (cur >= n) return;
+  long long guard = 4LL * n * n + 64;
+  while (cur >= 0) {
+    int p = ptr[cur];
+    const int L = len[cur];
+    const unsigned short *lc = list + (long long)cur * n;
+    int next = -1;
+    bool placed = false;
+    while (p < L && !placed) {
+      const int m = (L - p < SUITOR_BATCH) ? (L - p) : SUITOR_BATCH;
+      int xs[SUITOR_BATCH];
+      unsigned rk[SUITOR_BATCH], sw[SUITOR_BATCH];
+#pragma unroll
+      for (int i = 0; i < SUITOR_BATCH; ++i)
+        if (i < m) xs[i] = lc[p + i];
+#pragma unroll
+      for (int i = 0; i < SUITOR_BATCH; ++i)
+        if (i < m) {
+          rk[i] = rank[(long long)xs[i] * n + cur];
+          sw[i] = __ldcg(&suitor[xs[i]]);
+        }
+#pragma unroll
+      for (int i = 0; i < SUITOR_BATCH; ++i) {
+        if (i >= m || placed) continue;
+        unsigned old = sw[i];
+        while ((old >> 16) > rk[i]) {
+          if (--guard < 0) { atomicMin(&st->err, -40); return; }
+          ptr[cur] = p + i + 1;  // where a later search for cur resumes
+          __threadfence();
+          const unsigned prev = atomicCAS(&suitor[xs[i]], old, (rk[i] << 16) | (unsigned)cur);
+          if (prev == old) {
+            placed = true;
+            next = (old == SUITOR_EMPTY) ? -1 : (int)(old & 0xFFFFu);
+            break;
+          }
+          old = prev;
+        }
+        if (placed) p = p + i + 1;
+      }
+      if (!placed) p += m;
+      if (--guard < 0) { atomicMin(&st->err, -40); return; }
+    }
+    if (!placed) ptr[cur] = p;
+    __threadfence();
+    cur = next;
+  }
+}
+
+// the end of the previous step: SL := MIN(SL, NL) and the loop test
+// (src/D/dstep.F90:442, 564-583), with the statistics of DSTEP_TRANSF
+// (src/D/dstep.F90:349-370) when tracing
+template <typename T>
+__device__ void end_of_step(State *st, const Piv<T> *piv, const int *J, Trace &tr)
+{
+  if (!st->pending || st->stop) return;
+  st->pending = 0;
+  const int sl = st->sl, nl = st->nl, err = st->err;
+  if (st->trace_on) {
+    double tw = -0.0;
+    int tg = 0, hy = 0;
+    if (err == 0)
+      for (int i = 0; i < sl; ++i) {
+        const int l = piv[i].info;
+        if ((l & 2) || (l & 4)) {
+          tw = __dadd_rn(tw, piv[i].w);
+          if (J[piv[i].p] == J[piv[i].q]) ++tg; else ++hy;
+        }
+      }
+    if (st->trace_steps < st->trace_cap_steps) {
+      const int s = st->trace_steps++;
+      tr.sl[s] = sl; tr.nl[s] = (err < 0) ? err : nl; tr.tw[s] = tw; tr.trig[s] = tg; tr.hyp[s] = hy;
+    }
+    for (int i = 0; i < sl; ++i)
+      if (st->trace_npiv < st->trace_cap_piv) tr.piv[st->trace_npiv++] = make_int2(piv[i].p, piv[i].q);
+  }
+  if (err < 0) { st->info = err; st->stop = 1; }
+  else if (((sl < nl) ? sl : nl) <= 0) { st->info = st->steps; st->stop = 1; }
+  else st->steps += 1;
+}
+
+// one block: the matched pairs, their ranking, the first N_2 pivots, their 2x2 HSVDs (the
+// first loop of DSTEP_TRANSF, src/D/dstep.F90:301-326: INFO, NL, the BA coefficients
+// of V) and the columns outside the pivot set.  A == nullptr: selection only.
+template <typename T>
+__global__ void __launch_bounds__(SEL_THREADS, 1)
+k_select(State *st, const double *__restrict__ Wm, const T *__restrict__ A, const int *__restrict__ J, int n, int n_2,
+         const unsigned *suitor, Piv<T> *piv, RowRot<T> *rr, int *unp, Trace tr, int quirk)
+{
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int s2 = pow2ceil(n / 2 > 0 ? n / 2 : 1);
+  unsigned long long *skey = (unsigned long long *)smem_raw;  // [s2]
+  unsigned *stie = (unsigned *)(skey + s2);                   // [s2]
+  int *sidx = (int *)(stie + s2);                             // [s2]
+  int2 *pairs = (int2 *)(sidx + s2);                          // [n/2 + 1]
+  unsigned char *ms = (unsigned char *)(pairs + (n / 2 + 1)); // [n]
+  __shared__ int s_stop, s_cnt, s_nl, s_err, s_nunp;
+
+  const int tid = threadIdx.x, nth = blockDim.x;
+  if (tid == 0) {
+    end_of_step<T>(st, piv, J, tr);
+    s_stop = st->stop;
+    s_cnt = 0; s_nl = 0; s_err = 0; s_nunp = 0;
+  }
+  __syncthreads();
+  if (s_stop) return;
+  // the mutual suitor pairs are the matching
+  for (int v = tid; v < n; v += nth) {
+    const unsigned a = suitor[v];
+    if (a == SUITOR_EMPTY) continue;
+    const int u = (int)(a & 0xFFFFu);
+    const unsigned b = suitor[u];
+    if (v < u && b != SUITOR_EMPTY && (int)(b & 0xFFFFu) == v) pairs[atomicAdd(&s_cnt, 1)] = make_int2(v, u);
+  }
+  __syncthreads();
+
+  // rank the matched pairs: bitonic sort on (weight key, tie key), descending
+  const int np = s_cnt;
+  for (int i = tid; i < s2; i += nth) {
+    if (i < np) {
+      const int2 pr = pairs[i];
+      skey[i] = wkey(Wm[(long long)pr.x * n + pr.y]);
+      stie[i] = tkey(pr.x, pr.y);
+      sidx[i] = i;
+    }
+    else { skey[i] = 0ULL; stie[i] = 0u; sidx[i] = -1; }
+  }
+  __syncthreads();
+  bitonic_desc(skey, stie, sidx, s2);
+  const int sl = (np < n_2) ? np : n_2;
+
+  // the pivot set and the columns outside it
+  for (int v = tid; v < n; v += nth) ms[v] = 0;
+  __syncthreads();
+  for (int r = tid; r < sl; r += nth) {
+    const int2 pr = pairs[sidx[r]];
+    ms[pr.x] = 1;
+    ms[pr.y] = 1;
+  }
+  __syncthreads();
+  for (int v = tid; v < n; v += nth)
+    if (!ms[v]) unp[atomicAdd(&s_nunp, 1)] = v;
+
+  for (int r = tid; r < sl; r += nth) {
+    const int2 pr = pairs[sidx[r]];
+    Piv<T> &pv = piv[r];
+    pv.p = pr.x;
+    pv.q = pr.y;
+    pv.w = Wm[(long long)pr.x * n + pr.y];
+    if (!A) continue;
+    const int p = pr.x, q = pr.y;
+    T B[4] = { A[(long long)p * n + p], A[(long long)p * n + q], A[(long long)q * n + p], A[(long long)q * n + q] };
+    T V[4], W[4];
+    int info = 0;
+    Tr<T>::hsvd2(B, J[p], J[q], V, W, JK_TH1FIX, info);
+    pv.info = info;
+    RowRot<T> x;
+    x.p = p; x.q = q; x.flags = 0;
+    if (info >= 0) {
+#pragma unroll
+      for (int k = 0; k < 4; ++k) { pv.V[k] = V[k]; pv.W[k] = W[k]; }
+      pv.d[0] = Tr<T>::re(B[M11]);
+      pv.d[1] = Tr<T>::re(B[M22]);
+      if (info & 2) {
+        const typename Tr<T>::R t = Tr<T>::ba(V, quirk);
+        x.flags = (t.c1 ? 1 : 0) | (t.c2 ? 2 : 0) | 4;
+        x.r1 = t.r1; x.r2 = t.r2; x.m1 = t.m1; x.m2 = t.m2;
+      }
+      if ((info & 1) && (info & 6)) atomicAdd(&s_nl, 1);
+    }
+    else
+      atomicMin(&s_err, info);
+    rr[r] = x;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    st->sl = sl;
+    st->nl = s_nl;
+    st->err = s_err;
+    st->nunp = s_nunp;
+    if (sl <= 0) {
+      // DSTEP_EXEC returns with SL = 0: the loop ends with INFO = S (src/D/dstep.F90:421, 575-582)
+      st->info = st->steps;
+      st->stop = 1;
+      if (st->trace_on && st->trace_steps < st->trace_cap_steps) {
+        const int s = st->trace_steps++;
+        tr.sl[s] = 0; tr.nl[s] = -1; tr.tw[s] = -0.0; tr.trig[s] = 0; tr.hyp[s] = 0;
+      }
+    }
+    else st->pending = 1;
+  }
+}
+
+size_t select_smem(int n)
+{
+  const int s2 = pow2ceil(n / 2 > 0 ? n / 2 : 1);
+  return (size_t)s2 * (8 + 4 + 4) + (size_t)(n / 2 + 1) * 8 + (size_t)n + 16;
+}
+
+size_t colsort_smem(int n) { return (size_t)pow2ceil(n) * (8 + 4 + 4); }
+// ---------------------------------------------------------------------------
+// the fused transformations of one step (src/D/dstep.F90:301-346).
+// Block b < SL owns pivot b's column pair (p, q); the other blocks own two
+// columns outside the pivot set.  Each block: load its columns of A; apply the
+// row rotations of all pivots (BA of phase 1); then, for a pivot block and when no
+// pivot failed, the column rotation AB (phase 2) and the diagonal write-back; store;
+// then rotate the columns p, q of U (by V^T / V^H) and of Z (by W), phase 1.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(256)
+k_rotate(const State *st, T *__restrict__ A, T *__restrict__ U, T *__restrict__ Z, int n, const Piv<T> *__restrict__ piv,
+         const RowRot<T> *__restrict__ rr, const int *__restrict__ unp)
+{
+  if (st->stop) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T *col = (T *)smem_raw;
+  const int sl = st->sl, b = blockIdx.x;
+  int c0, c1 = -1, k = -1;
+  if (b < sl) { k = b; c0 = piv[k].p; c1 = piv[k].q; }
+  else {
+    const int j = 2 * (b - sl), nu = st->nunp;
+    if (j >= nu) return;
+    c0 = unp[j];
+    if (j + 1 < nu) c1 = unp[j + 1];
+  }
+  T *A0 = A + (long long)c0 * n, *A1 = (c1 >= 0) ? (A + (long long)c1 * n) : nullptr;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    col[i] = A0[i];
+    if (A1) col[n + i] = A1[i];
+  }
+  __syncthreads();
+  // phase 1: rows p_m, q_m of every pivot m (BA)
+  for (int m = threadIdx.x; m < sl; m += blockDim.x) {
+    const RowRot<T> r = rr[m];
+    if (!(r.flags & 4)) continue;
+    typename Tr<T>::R t;
+    t.c1 = r.flags & 1; t.c2 = (r.flags >> 1) & 1;
+    t.r1 = r.r1; t.r2 = r.r2; t.m1 = r.m1; t.m2 = r.m2;
+    Tr<T>::apply_ba(t, col[r.p], col[r.q]);
+    if (A1) Tr<T>::apply_ba(t, col[n + r.p], col[n + r.q]);
+  }
+  __syncthreads();
+  // phase 2 for the pivot's own column pair, only when no pivot failed
+  if (k >= 0 && st->err == 0) {
+    const Piv<T> &pv = piv[k];
+    const int info = pv.info;
+    if (info & 4) {
+      T W[4] = { pv.W[0], pv.W[1], pv.W[2], pv.W[3] };
+      const typename Tr<T>::R t = Tr<T>::ab(W);
+      for (int i = threadIdx.x; i < n; i += blockDim.x) Tr<T>::apply_ab(t, col[i], col[n + i]);
+    }
+    __syncthreads();
+    if (!(info & 8) && threadIdx.x == 0) {
+      T d0 = Tr<T>::zero(), d1 = Tr<T>::zero();
+      if constexpr (sizeof(T) == sizeof(double)) { *(double *)&d0 = pv.d[0]; *(double *)&d1 = pv.d[1]; }
+      else { ((double2 *)&d0)->x = pv.d[0]; ((double2 *)&d1)->x = pv.d[1]; }
+      col[c0] = d0;                   // A(p,p)
+      col[c1] = Tr<T>::zero();        // A(q,p)
+      col[n + c0] = Tr<T>::zero();    // A(p,q)
+      col[n + c1] = d1;               // A(q,q)
+    }
+    __syncthreads();
+  }
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    A0[i] = col[i];
+    if (A1) A1[i] = col[n + i];
+  }
+  if (k < 0) return;
+  const Piv<T> &pv = piv[k];
+  const int info = pv.info;
+  if (info < 0) return;
+  if (info & 2) {
+    T V[4] = { pv.V[0], pv.V[1], pv.V[2], pv.V[3] };
+    Tr<T>::ut2(V);
+    const typename Tr<T>::R t = Tr<T>::ab(V);
+    T *u0 = U + (long long)c0 * n, *u1 = U + (long long)c1 * n;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      T x = u0[i], y = u1[i];
+      Tr<T>::apply_ab(t, x, y);
+      u0[i] = x; u1[i] = y;
+    }
+  }
+  if (info & 4) {
+    T W[4] = { pv.W[0], pv.W[1], pv.W[2], pv.W[3] };
+    const typename Tr<T>::R t = Tr<T>::ab(W);
+    T *z0 = Z + (long long)c0 * n, *z1 = Z + (long long)c1 * n;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      T x = z0[i], y = z1[i];
+      Tr<T>::apply_ab(t, x, y);
+      z0[i] = x; z1[i] = y;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// a batch of independent 2x2 HSVDs (the dtest / ztest kernel, src/D/dtest.F90:35)
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void k_hsvd2_batch(int count, T *A, const int *J, T *U, T *Z, int *info, double th1)
+{
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= count) return;
+  T a[4], u[4], z[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) a[k] = A[4 * i + k];
+  int inf = 0;
+  Tr<T>::hsvd2(a, J[2 * i], J[2 * i + 1], u, z, th1, inf);
+#pragma unroll
+  for (int k = 0; k < 4; ++k) { A[4 * i + k] = a[k]; U[4 * i + k] = u[k]; Z[4 * i + k] = z[k]; }
+  info[i] = inf;
+}
+
+// ---------------------------------------------------------------------------
+// host launchers
+// ---------------------------------------------------------------------------
+static int grid1(long long work, int threads)
+{
+  long long g = (work + threads - 1) / threads;
+  if (g < 1) g = 1;
+  if (g > 148LL * 64) g = 148LL * 64;
+  return (int)g;
+}
+
+cudaError_t prepare_kernels(int n)
+{
+  // dynamic shared memory beyond the default 48 KB: two columns of A per k_rotate
+  // block, the ranking and matching state of k_select
+  cudaError_t e = cudaFuncSetAttribute(k_rotate<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * n * 8);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_rotate<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * n * 16);
+  const int ss = (int)select_smem(n);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_colsort, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)colsort_smem(n));
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_select<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, ss);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_select<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, ss);
+  return e;
+}
+
+template <typename T>
+static cudaError_t init_t(Workspace &w, T *U, T *Z, cudaStream_t s)
+{
+  k_state_init<<<1, 1, 0, s>>>(w.st);
+  k_identity2<T><<<grid1((long long)w.n * w.n, 256), 256, 0, s>>>(U, Z, w.n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_init(Workspace &w, void *U, void *Z, cudaStream_t s)
+{
+  return w.cplx ? init_t(w, (double2 *)U, (double2 *)Z, s) : init_t(w, (double *)U, (double *)Z, s);
+}
+
+template <typename T>
+static cudaError_t weights_t(Workspace &w, const T *A, cudaStream_t s)
+{
+  const int n = w.n;
+  dim3 bt(32, 8), gt((n + 31) / 32, (n + 7) / 8);
+  k_weights_trig<T><<<gt, bt, 0, s>>>(w.st, A, w.J, w.Wm, n);
+  if (w.n_plus > 0 && w.n_minus > 0) {
+    // 16 x 16 pair tiles once they fill the GPU, 8 x 8 below
+    if ((long long)w.n_plus * w.n_minus >= 256LL * 148 * 4) {
+      dim3 gh((w.n_plus + 15) / 16, (w.n_minus + 15) / 16);
+      k_weights_hyp<T, 16, 16><<<gh, 256, 0, s>>>(w.st, A, w.plus, w.minus, w.n_plus, w.n_minus, w.Wm, n);
+    }
+    else {
+      dim3 gh((w.n_plus + 7) / 8, (w.n_minus + 7) / 8);
+      k_weights_hyp<T, 8, 8><<<gh, 64, 0, s>>>(w.st, A, w.plus, w.minus, w.n_plus, w.n_minus, w.Wm, n);
+    }
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_weights(Workspace &w, const void *A, cudaStream_t s)
+{
+  return w.cplx ? weights_t(w, (const double2 *)A, s) : weights_t(w, (const double *)A, s);
+}
+
+template <typename T>
+static cudaError_t select_t(Workspace &w, const T *A, int n_2, cudaStream_t s)
+{
+  const int n = w.n;
+  k_colsort<<<n, SORT_THREADS, colsort_smem(n), s>>>(w.st, w.Wm, n, w.list, w.rank, w.len, w.ptr, w.suitor);
+  k_suitor<<<(n + 127) / 128, 128, 0, s>>>(w.st, n, w.list, w.rank, w.len, w.ptr, w.suitor);
+  k_select<T><<<1, SEL_THREADS, select_smem(n), s>>>(w.st, w.Wm, A, w.J, n, n_2, w.suitor, (Piv<T> *)w.piv,
+                                                     (RowRot<T> *)w.rowrot, w.unp, w.tr, w.zba_quirk);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_match(Workspace &w, int n_2, cudaStream_t s)
+{
+  return select_t<double>(w, (const double *)nullptr, n_2, s);
+}
+
+template <typename T>
+static cudaError_t step_t(Workspace &w, T *A, T *U, T *Z, int n_2, cudaStream_t s)
+{
+  const int n = w.n;
+  cudaError_t e = weights_t(w, (const T *)A, s);
+  if (e != cudaSuccess) return e;
+  e = select_t(w, (const T *)A, n_2, s);
+  if (e != cudaSuccess) return e;
+  k_rotate<T><<<(n + 1) / 2, 256, 2 * (size_t)n * sizeof(T), s>>>(w.st, A, U, Z, n, (const Piv<T> *)w.piv,
+                                                                 (const RowRot<T> *)w.rowrot, w.unp);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_step(Workspace &w, void *A, void *U, void *Z, int n_2, cudaStream_t s)
+{
+  return w.cplx ? step_t(w, (double2 *)A, (double2 *)U, (double2 *)Z, n_2, s)
+                : step_t(w, (double *)A, (double *)U, (double *)Z, n_2, s);
+}
+
+template <typename T>
+static cudaError_t finish_t(Workspace &w, T *A, T *Z, double *sigma, cudaStream_t s)
+{
+  const int n = w.n, nt = (n + 31) / 32;
+  k_sigma<T><<<grid1(n, 256), 256, 0, s>>>(A, sigma, n);
+  k_jztj<T><<<nt * (nt + 1) / 2, dim3(32, 8), 0, s>>>(Z, w.J, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_finish(Workspace &w, void *A, void *Z, double *sigma, cudaStream_t s)
+{
+  return w.cplx ? finish_t(w, (double2 *)A, (double2 *)Z, sigma, s) : finish_t(w, (double *)A, (double *)Z, sigma, s);
+}
+
+cudaError_t launch_hsvd2_batch(int cplx, int count, void *A, const int *J, void *U, void *Z, int *info, double th1, cudaStream_t s)
+{
+  if (count <= 0) return cudaSuccess;
+  if (cplx) k_hsvd2_batch<double2><<<(count + 127) / 128, 128, 0, s>>>(count, (double2 *)A, J, (double2 *)U, (double2 *)Z, info, th1);
+  else k_hsvd2_batch<double><<<(count + 127) / 128, 128, 0, s>>>(count, (double *)A, J, (double *)U, (double *)Z, info, th1);
+  return cudaGetLastError();
+}
+
+}  // namespace jk

@@ -63,6 +63,7 @@ def lib():
         L.jo_jstep_len.restype = C.c_int
         L.jo_jstep_len.argtypes = [C.c_int, C.c_int]
         L.jo_set_zba_quirk.argtypes = [C.c_int]
+        L.jo_set_max_steps.argtypes = [C.c_int]
         _lib = L
     return _lib
 
@@ -103,7 +104,7 @@ def _collect(tr, bufs):
                 piv=bufs["piv"][:2 * tr.n_piv].reshape(-1, 2).copy())
 
 
-def step_loop(Y, J, n_2=0, id_ncp=0, id_tru=0, nt=1, trace=False, max_steps=1 << 16, max_piv=1 << 24):
+def step_loop(Y, J, n_2=0, id_ncp=0, id_tru=0, nt=1, trace=False, max_steps=1 << 16, max_piv=1 << 24, stop_after=0):
     """Run the oracle's DSTEP_LOOP / ZSTEP_LOOP on a copy of Y (real or complex, n x n).
 
     Returns a dict with info, A (the matrix after the loop, diagonal zeroed as the
@@ -123,8 +124,10 @@ def step_loop(Y, J, n_2=0, id_ncp=0, id_tru=0, nt=1, trace=False, max_steps=1 <<
     if trace:
         trp, bufs = _new_trace(max_steps, max_piv)
     fn = L.jo_zstep_loop if cplx else L.jo_dstep_loop
+    L.jo_set_max_steps(int(stop_after))
     info = fn(n, _dp(U), n, _dp(A), n, _dp(Z), n, _ip(Jc), _dp(s), int(n_2), int(id_ncp), int(id_tru), int(nt),
               C.byref(trp) if trace else None)
+    L.jo_set_max_steps(0)
     out = dict(info=info, A=A, U=U, Z=Z, sigma=s)
     if trace:
         out["trace"] = _collect(trp, bufs)

@@ -966,6 +966,11 @@ static void jo_trace_step(jo_trace *tr, int sl, int nl, const double st[3], cons
   ++tr->n_steps;
 }
 
+/* optional stop after a number of steps (tests and experiments only; 0 = none) */
+static int jo_max_steps = 0;
+void jo_set_max_steps(int m) { jo_max_steps = (m > 0) ? m : 0; }
+int jo_get_max_steps(void) { return jo_max_steps; }
+
 /* DSTEP_LOOP (with DSTEP_EXEC and JZTJ), src/D/dstep.F90:376-604 */
 int jo_dstep_loop(int n, double *U, int ldu, double *A, int lda, double *Z, int ldz,
                   const int *J, double *sigma, int n_2, int id_ncp, int id_tru, int nt, jo_trace *tr)
@@ -1014,6 +1019,7 @@ int jo_dstep_loop(int n, double *U, int ldu, double *A, int lda, double *Z, int 
     sl = (sl < nl) ? sl : nl;
     if (sl <= 0) break;
     ++s;
+    if (jo_max_steps && s >= jo_max_steps) break;
   }
   if (sl < 0) info = sl;
   else if (info >= 0) info = s;

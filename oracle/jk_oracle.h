@@ -98,6 +98,9 @@ int jo_zstep_loop(int n, jo_z *U, int ldu, jo_z *A, int lda, jo_z *Z, int ldz,
                   const int *J, double *sigma, int n_2, int id_ncp, int id_tru, int nt,
                   jo_trace *tr);
 
+/* Stop every later loop after m steps (0: run to convergence); test helper. */
+void jo_set_max_steps(int m);
+
 /* One build phase alone: weights of all pairs in the reference's record order
  * (TRU1/TRU2), NaN where the reference stores a NaN. w must hold NN doubles.
  * Returns TT (number of trigonometric pairs) or < 0. */

@@ -508,6 +508,7 @@ static int jo_zstep_transf(int n, jo_z *U, int ldu, jo_z *A, int lda, jo_z *Z, i
 }
 
 void jo_trace_step_shared(jo_trace *tr, int sl, int nl, const double st[3], const jo_aw *dz, const int *step);
+int jo_get_max_steps(void);
 
 /* ZSTEP_LOOP (with ZSTEP_EXEC and JZHJ), src/Z/zstep.F90:379-615 */
 int jo_zstep_loop(int n, jo_z *U, int ldu, jo_z *A, int lda, jo_z *Z, int ldz,
@@ -557,6 +558,7 @@ int jo_zstep_loop(int n, jo_z *U, int ldu, jo_z *A, int lda, jo_z *Z, int ldz,
     sl = (sl < nl) ? sl : nl;
     if (sl <= 0) break;
     ++s;
+    if (jo_get_max_steps() && s >= jo_get_max_steps()) break;
   }
   if (sl < 0) info = sl;
   else if (info >= 0) info = s;

@@ -1,0 +1,49 @@
+"""The C ABI library loads and exports every entry point include/jkogb.h declares (no GPU needed)."""
+import ctypes
+import os
+import re
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared():
+    src = open(os.path.join(ROOT, "include", "jkogb.h")).read()
+    return sorted(set(re.findall(r"\b(jk_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_header_and_python_agree():
+    import jkogb_b200
+    assert sorted(jkogb_b200.SYMBOLS) == _declared()
+
+
+def test_library_exports_all_symbols():
+    from jkogb_b200.build import build
+    path = build()
+    L = ctypes.CDLL(path)
+    for name in _declared():
+        assert hasattr(L, name), name
+
+
+def test_argument_errors_without_gpu():
+    # argument checks run before any CUDA call
+    import numpy as np
+    import jkogb_b200 as jk
+    L = jk.lib()
+    n = 4
+    A = np.zeros((n, n))
+    J = np.array([1, 1, -1, 2], np.int32)
+    o = jk.Opts()
+    d = lambda a: a.ctypes.data  # noqa: E731
+    Jp = J.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+    assert L.jk_dstep_loop(2, d(A), n, d(A), n, d(A), n, Jp, d(A), 0, 0, 0, ctypes.byref(o), None) == -1
+    assert L.jk_dstep_loop(n, d(A), 3, d(A), n, d(A), n, Jp, d(A), 0, 0, 0, ctypes.byref(o), None) == -3
+    assert L.jk_dstep_loop(n, d(A), n, d(A), 3, d(A), n, Jp, d(A), 0, 0, 0, ctypes.byref(o), None) == -5
+    assert L.jk_dstep_loop(n, d(A), n, d(A), n, d(A), 2, Jp, d(A), 0, 0, 0, ctypes.byref(o), None) == -7
+    assert L.jk_dstep_loop(n, d(A), n, d(A), n, d(A), n, Jp, d(A), -1, 0, 0, ctypes.byref(o), None) == -16
+    assert L.jk_dstep_loop(n, d(A), n, d(A), n, d(A), n, Jp, d(A), 0, 4, 0, ctypes.byref(o), None) == -21
+    assert L.jk_dstep_loop(n, d(A), n, d(A), n, d(A), n, Jp, d(A), 0, 0, 3, ctypes.byref(o), None) == -22
+    assert L.jk_dstep_loop(n, d(A), n, d(A), n, d(A), n, Jp, d(A), 0, 0, 0, ctypes.byref(o), None) == -23
+    assert jk.jstep_len(7, 0) == 3 and jk.jstep_len(7, 9) == 3 and jk.jstep_len(7, 2) == 2
+    assert "J" in jk.strerror(-23)
