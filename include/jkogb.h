@@ -40,9 +40,10 @@ typedef struct {
  * the selected pivots of every step (the AW_OUT dump, src/shared/atypes.F90:30-77).
  * Host buffers sized by the caller; unused pointers may be NULL. */
 typedef struct {
-  int max_steps;        /* capacity of sl/nl/trig/hyp/tw */
+  int max_steps;        /* capacity of sl/nl/trig/hyp/tw/rounds */
   int *sl, *nl, *trig, *hyp;
   double *tw;
+  int *rounds;          /* matching rounds of the selection of each step (telemetry) */
   long long max_piv;    /* capacity of piv in pivots */
   int *piv;             /* 2 ints per pivot: p, q (1-based), in selection order, all steps */
   long long n_piv;      /* out */
@@ -92,6 +93,24 @@ int jk_zweights(int n, const double *A, int lda, const int *J, double *W);
  * src/shared/atypes.F90:85-484) on the device, from a symmetric n x n host weight
  * matrix; writes SL pivots (1-based p < q) in selection order and returns SL. */
 int jk_select(int n, const double *W, int n_2, int *piv);
+
+/* A reusable device workspace for one order N and sign vector J (kernel-level use). */
+typedef struct jk_handle jk_handle;
+jk_handle *jk_handle_create(int n, int complex_, const int *J, int *info);
+void jk_handle_destroy(jk_handle *h);
+
+/* Enqueue one build's pair weights (the two weight kernels) of the device matrix dA
+ * (leading dimension n) on `stream`; when dW is not NULL, also copy the symmetric
+ * n x n weight matrix there (device pointer).  Returns 0 or an INFO error. */
+int jk_handle_weights(jk_handle *h, const double *dA, double *dW, void *stream);
+
+/* Kernel launches enqueued by the calling thread's last step-loop call. */
+long long jk_last_launch_count(void);
+
+/* FP64 FMA throughput of the current device in TFLOP/s (2 flops per fma), from a
+ * dependent-chain kernel with 8 chains per thread over a full grid; the peak the
+ * FP64 roofline is quoted against. */
+double jk_fp64_peak(void);
 
 /* Largest order N the loops accept. */
 int jk_max_order(int complex_);

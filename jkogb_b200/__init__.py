@@ -29,7 +29,8 @@ LIB_PATH = os.path.join(_HERE, "_lib", "libjkogb_b200.so")
 
 # every symbol include/jkogb.h declares
 SYMBOLS = ("jk_dstep_loop", "jk_zstep_loop", "jk_dstep_loop_dev", "jk_zstep_loop_dev", "jk_dhsvd2_batch",
-           "jk_zhsvd2_batch", "jk_dweights", "jk_zweights", "jk_select", "jk_max_order", "jk_strerror")
+           "jk_zhsvd2_batch", "jk_dweights", "jk_zweights", "jk_select", "jk_handle_create", "jk_handle_destroy",
+           "jk_handle_weights", "jk_last_launch_count", "jk_fp64_peak", "jk_max_order", "jk_strerror")
 
 
 class JkError(RuntimeError):
@@ -48,8 +49,8 @@ class Opts(C.Structure):
 class Trace(C.Structure):
     _fields_ = [("max_steps", C.c_int), ("sl", C.POINTER(C.c_int)), ("nl", C.POINTER(C.c_int)),
                 ("trig", C.POINTER(C.c_int)), ("hyp", C.POINTER(C.c_int)), ("tw", C.POINTER(C.c_double)),
-                ("max_piv", C.c_longlong), ("piv", C.POINTER(C.c_int)), ("n_piv", C.c_longlong),
-                ("n_steps", C.c_int)]
+                ("rounds", C.POINTER(C.c_int)), ("max_piv", C.c_longlong), ("piv", C.POINTER(C.c_int)),
+                ("n_piv", C.c_longlong), ("n_steps", C.c_int)]
 
 
 _lib = None
@@ -82,6 +83,16 @@ def lib():
             f.argtypes = [C.c_int, vp, C.c_int, ip, dp]
         L.jk_select.restype = C.c_int
         L.jk_select.argtypes = [C.c_int, dp, C.c_int, ip]
+        L.jk_handle_create.restype = C.c_void_p
+        L.jk_handle_create.argtypes = [C.c_int, C.c_int, ip, ip]
+        L.jk_handle_destroy.restype = None
+        L.jk_handle_destroy.argtypes = [C.c_void_p]
+        L.jk_handle_weights.restype = C.c_int
+        L.jk_handle_weights.argtypes = [C.c_void_p, vp, vp, vp]
+        L.jk_last_launch_count.restype = C.c_longlong
+        L.jk_last_launch_count.argtypes = []
+        L.jk_fp64_peak.restype = C.c_double
+        L.jk_fp64_peak.argtypes = []
         L.jk_max_order.restype = C.c_int
         L.jk_max_order.argtypes = [C.c_int]
         L.jk_strerror.restype = C.c_char_p
@@ -111,9 +122,9 @@ def _new_trace(max_steps, max_piv):
     tr = Trace()
     bufs = dict(sl=np.zeros(max_steps, np.int32), nl=np.zeros(max_steps, np.int32), trig=np.zeros(max_steps, np.int32),
                 hyp=np.zeros(max_steps, np.int32), tw=np.zeros(max_steps, np.float64),
-                piv=np.zeros(2 * max_piv, np.int32))
+                rounds=np.zeros(max_steps, np.int32), piv=np.zeros(2 * max_piv, np.int32))
     tr.max_steps, tr.max_piv = max_steps, max_piv
-    for k in ("sl", "nl", "trig", "hyp", "piv"):
+    for k in ("sl", "nl", "trig", "hyp", "rounds", "piv"):
         setattr(tr, k, bufs[k].ctypes.data_as(C.POINTER(C.c_int)))
     tr.tw = bufs["tw"].ctypes.data_as(C.POINTER(C.c_double))
     return tr, bufs
@@ -122,7 +133,8 @@ def _new_trace(max_steps, max_piv):
 def _collect(tr, bufs):
     m = min(tr.n_steps, len(bufs["sl"]))
     return dict(n_steps=tr.n_steps, sl=bufs["sl"][:m].copy(), nl=bufs["nl"][:m].copy(), trig=bufs["trig"][:m].copy(),
-                hyp=bufs["hyp"][:m].copy(), tw=bufs["tw"][:m].copy(), piv=bufs["piv"][:2 * tr.n_piv].reshape(-1, 2).copy())
+                hyp=bufs["hyp"][:m].copy(), tw=bufs["tw"][:m].copy(), rounds=bufs["rounds"][:m].copy(),
+                piv=bufs["piv"][:2 * tr.n_piv].reshape(-1, 2).copy())
 
 
 def step_loop(Y, J, n_2=0, id_ncp=0, id_tru=0, trace=False, max_steps=0, zba_quirk=0, graph_steps=0,
@@ -218,6 +230,36 @@ def weights(A, J):
     if rc < 0:
         raise JkError(rc, "weights: ")
     return W
+
+
+class Handle:
+    """A device workspace for one order n and sign vector J (kernel-level entry points)."""
+
+    def __init__(self, n, J, complex_=False):
+        Jc = np.ascontiguousarray(np.asarray(J, np.int32))
+        info = C.c_int(0)
+        self.n = int(n)
+        self._h = lib().jk_handle_create(self.n, int(bool(complex_)), Jc.ctypes.data_as(C.POINTER(C.c_int)),
+                                          C.byref(info))
+        if not self._h:
+            raise JkError(info.value, "handle: ")
+
+    def weights(self, dA_ptr, dW_ptr=None, stream=0):
+        """Enqueue one build's weights of the device matrix at dA_ptr on `stream` (a raw cudaStream_t)."""
+        rc = lib().jk_handle_weights(self._h, C.c_void_p(dA_ptr), C.c_void_p(dW_ptr or 0), C.c_void_p(stream))
+        if rc < 0:
+            raise JkError(rc, "handle weights: ")
+
+    def close(self):
+        if self._h:
+            lib().jk_handle_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def select(W, n_2):

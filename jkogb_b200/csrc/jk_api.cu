@@ -13,6 +13,8 @@ using namespace jk;
 
 namespace {
 
+thread_local long long g_launches = 0;
+
 struct Guard {
   std::vector<void *> dev;
   void *pinned = nullptr;
@@ -45,7 +47,7 @@ int max_order(int cplx)
   // k_rotate keeps two columns of A in shared memory and k_select its matching state
   // (227 KB per block each); the tie key packs p in 16 bits
   int n = (227 * 1024) / (2 * (cplx ? 16 : 8));
-  while (n > 3 && (select_smem(n) > 227 * 1024 || colsort_smem(n) > 227 * 1024)) --n;
+  while (n > 3 && (select_smem(n) > 227 * 1024 || colsort_e(n) > 16)) --n;
   return n < 65535 ? n : 65535;
 }
 
@@ -94,13 +96,16 @@ int make_workspace(Guard &g, Workspace &w, int n, int cplx, const int *J, int tr
   CK(g.alloc(&w.plus, (plus.size() + 1) * sizeof(int)));
   CK(g.alloc(&w.minus, (minus.size() + 1) * sizeof(int)));
   CK(g.alloc(&w.Wm, (size_t)n * n * sizeof(double)));
+  {
+    const size_t T = (n + 31) / 32, nt = T * (T + 1) / 2;
+    CK(g.alloc(&w.hpar, nt * 1024 * sizeof(HypPar)));
+    CK(g.alloc(&w.tcount, nt * sizeof(int)));
+  }
   CK(g.alloc(&w.piv, half * pivsz));
   CK(g.alloc(&w.rowrot, half * rrsz));
-  CK(g.alloc(&w.list, (size_t)n * n * sizeof(unsigned short)));
+  CK(g.alloc(&w.list, (size_t)n * ((n + 7) & ~7) * sizeof(unsigned short)));
   CK(g.alloc(&w.rank, (size_t)n * n * sizeof(unsigned short)));
   CK(g.alloc(&w.len, n * sizeof(int)));
-  CK(g.alloc(&w.ptr, n * sizeof(int)));
-  CK(g.alloc(&w.suitor, n * sizeof(unsigned)));
   CK(g.alloc(&w.unp, (n + 1) * sizeof(int)));
   CK(g.alloc(&w.st, sizeof(State)));
   if (trace_on) {
@@ -111,6 +116,7 @@ int make_workspace(Guard &g, Workspace &w, int n, int cplx, const int *J, int tr
     CK(g.alloc(&w.tr.trig, cs * sizeof(int)));
     CK(g.alloc(&w.tr.hyp, cs * sizeof(int)));
     CK(g.alloc(&w.tr.tw, cs * sizeof(double)));
+    CK(g.alloc(&w.tr.rounds, cs * sizeof(int)));
     CK(g.alloc(&w.tr.piv, cp * sizeof(int2)));
   }
   CK(cudaMallocHost((void **)&g.pinned, sizeof(State)));
@@ -145,6 +151,7 @@ int run_loop(int cplx, int n, void *dU, void *dA, void *dZ, const int *J, double
   if (rc) return rc;
   w.zba_quirk = (o.zba_quirk == 0) ? 1 : 0;
 
+  g_launches = 2;  // state init, U = Z = I
   CK(launch_init(w, dU, dZ, s));
   int chunk = (o.graph_steps == 0) ? 32 : o.graph_steps;
   cudaGraphExec_t exec = nullptr;
@@ -182,10 +189,12 @@ int run_loop(int cplx, int n, void *dU, void *dA, void *dZ, const int *J, double
       return cuda_fail(e);
     }
     launched += per_sync;
+    g_launches += (long long)per_sync * (kStepLaunches - ((w.n_plus > 0 && w.n_minus > 0) ? 0 : 1));
     if (w.st_host->stop) { info = w.st_host->info; break; }
     if (w.st_host->steps >= cap || launched > 2 * cap + per_sync) { info = JK_ERR_MAX_STEPS; break; }
   }
   if (exec) cudaGraphExecDestroy(exec);
+  g_launches += 2;  // sigma, J Z^T J
   CK(launch_finish(w, dA, dZ, dsigma, s));
   if (trace) {
     const State &h = *w.st_host;
@@ -197,6 +206,7 @@ int run_loop(int cplx, int n, void *dU, void *dA, void *dZ, const int *J, double
       if (trace->trig) CK(cudaMemcpyAsync(trace->trig, w.tr.trig, ns * sizeof(int), cudaMemcpyDeviceToHost, s));
       if (trace->hyp) CK(cudaMemcpyAsync(trace->hyp, w.tr.hyp, ns * sizeof(int), cudaMemcpyDeviceToHost, s));
       if (trace->tw) CK(cudaMemcpyAsync(trace->tw, w.tr.tw, ns * sizeof(double), cudaMemcpyDeviceToHost, s));
+      if (trace->rounds) CK(cudaMemcpyAsync(trace->rounds, w.tr.rounds, ns * sizeof(int), cudaMemcpyDeviceToHost, s));
     }
     const long long np = h.trace_npiv < trace->max_piv ? h.trace_npiv : trace->max_piv;
     trace->n_piv = np;
@@ -361,6 +371,44 @@ int jk_select(int n, const double *W, int n_2, int *piv)
   if (sl > 0) CK(cudaMemcpy(pv.data(), w.piv, sl * sizeof(Piv<double>), cudaMemcpyDeviceToHost));
   for (int i = 0; i < sl; ++i) { piv[2 * i] = pv[i].p + 1; piv[2 * i + 1] = pv[i].q + 1; }
   return sl;
+}
+
+struct jk_handle {
+  Guard g;
+  Workspace w;
+};
+
+jk_handle *jk_handle_create(int n, int complex_, const int *J, int *info)
+{
+  int rc = check_args(n, n, n, n, J, 0, 0, 0, complex_ ? 1 : 0);
+  if (!rc) rc = pick_device(nullptr);
+  jk_handle *h = nullptr;
+  if (!rc) {
+    h = new jk_handle;
+    rc = make_workspace(h->g, h->w, n, complex_ ? 1 : 0, J, 0, 0, 0);
+    if (rc) { delete h; h = nullptr; }
+  }
+  if (info) *info = rc;
+  return h;
+}
+
+void jk_handle_destroy(jk_handle *h) { delete h; }
+
+int jk_handle_weights(jk_handle *h, const double *dA, double *dW, void *stream)
+{
+  if (!h || !dA) return -1;
+  cudaStream_t s = (cudaStream_t)stream;
+  CK(launch_weights(h->w, dA, s));
+  if (dW) CK(cudaMemcpyAsync(dW, h->w.Wm, (size_t)h->w.n * h->w.n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  return 0;
+}
+
+long long jk_last_launch_count(void) { return g_launches; }
+
+double jk_fp64_peak(void)
+{
+  if (pick_device(nullptr)) return -1.0;
+  return fp64_peak();
 }
 
 int jk_max_order(int complex_) { return max_order(complex_ ? 1 : 0); }

@@ -30,7 +30,7 @@ struct State {
 
 // Per-step trace on the device (optional).
 struct Trace {
-  int *sl, *nl, *trig, *hyp;
+  int *sl, *nl, *trig, *hyp, *rounds;
   double *tw;
   int2 *piv;  // 0-based (p, q)
 };
@@ -52,6 +52,14 @@ struct RowRot {
   T r1, r2, m1, m2;
 };
 
+// scan parameters of one hyperbolic pair (real path)
+struct HypPar {
+  double r1, r2, m1, m2, d;  // the AB coefficients of Z2 and the two leading terms
+  int p, q;                  // the pair (0-based, p < q)
+  int flags;                 // bit0 scan, bit1 c1, bit2 c2
+  int pad;
+};
+
 struct Workspace {
   int n;
   int cplx;
@@ -59,13 +67,13 @@ struct Workspace {
   int *J;            // signs (device)
   int *plus, *minus; // indices with J=+1 / J=-1, ascending
   double *Wm;        // n x n pair weights, symmetric, NaN = no transformation
+  void *hpar;        // per hyperbolic pair: scan parameters (real path), 1024 slots per 32 x 32 tile
+  int *tcount;       // hyperbolic pairs per tile
   void *piv;         // Piv<T>[n/2]
   void *rowrot;      // RowRot<T>[n/2]
-  unsigned short *list;  // n x n: the partners of every vertex, best first
+  unsigned short *list;  // n x list_ld(n): the partners of every vertex, best first
   unsigned short *rank;  // n x n: rank[v][u] = position of u in v's list
   int *len;              // valid entries of each list
-  int *ptr;              // resume position of each vertex's proposals
-  unsigned *suitor;      // (rank << 16 | vertex) of each vertex's current suitor
   int *unp;              // columns outside the current pivot set
   State *st;         // device state
   State *st_host;    // pinned host mirror
@@ -81,7 +89,10 @@ cudaError_t launch_weights(Workspace &w, const void *A, cudaStream_t s);
 cudaError_t launch_match(Workspace &w, int n_2, cudaStream_t s);
 cudaError_t launch_hsvd2_batch(int cplx, int count, void *A, const int *J, void *U, void *Z, int *info, double th1, cudaStream_t s);
 cudaError_t prepare_kernels(int n);
+double fp64_peak();
+// kernel launches of one step (the graph body)
+constexpr int kStepLaunches = 6;
 size_t select_smem(int n);
-size_t colsort_smem(int n);
+int colsort_e(int n);
 
 }  // namespace jk

@@ -1,23 +1,25 @@
 // jk_kernels.cu -- the per-step CUDA kernels of the J-Kogbetliantz HSVD (real and
 // complex), B200 (sm_100a).  One step of DSTEP_EXEC / ZSTEP_EXEC
-// (src/D/dstep.F90:376-443, src/Z/zstep.F90:379-447) is six launches:
+// (src/D/dstep.F90:376-443, src/Z/zstep.F90:379-447) is seven launches:
 //
 //   k_weights_trig  pair weights of the trigonometric pairs      (DMAGF2T / ZMAGF2T)
 //   k_weights_hyp   pair weights of the hyperbolic pairs         (DMAGF2H / ZMAGF2H)
 //                   = batched 2x2 HSVD + the tiled off-norm scan (ABODNDF2 / ABODNZF2)
 //   k_colsort       every vertex's partners ranked by the records' sort order (AW_CMP)
-//   k_suitor        the greedy non-colliding selection (AW_SRT* + AW_NCP1/2) as the
-//                   greedy matching, by lock-free suitor proposals
 //   k_select        one block: the end-of-step test of the previous step
-//                   (SL := MIN(SL, NL)), the ranking of the matched pairs, the first
-//                   N_2 of them, and the 2x2 HSVD of every selected pivot
-//                   (DHSVD2 / ZHSVD2) with INFO and NL
+//                   (SL := MIN(SL, NL)); the greedy non-colliding selection of the
+//                   sorted records (AW_SRT* + AW_NCP1/2) as the greedy matching, in
+//                   rounds of mutual best proposals; the ranking of the matched pairs
+//                   and the first N_2 of them
+//   k_pivots        the 2x2 HSVD of every selected pivot (DHSVD2 / ZHSVD2), INFO, NL
 //   k_rotate        fused transformations: every block loads a column pair of A,
 //                   applies all row rotations (BA), then its column rotation (AB)
 //                   and the diagonal write-back, and rotates the columns of U and Z
 //
 // Matrices are column-major with leading dimension n; complex entries are double2.
 #include <cooperative_groups.h>
+
+#include <cstdlib>
 
 #include "jk_internal.h"
 #include "jk_math.cuh"
@@ -250,6 +252,255 @@ __device__ __forceinline__ void scan_rows_cplx(const double2 *xs, const double2 
   }
 }
 
+// ---------------------------------------------------------------------------
+// the real hyperbolic weights, pipelined: a block owns 16 "+" columns x 32 "-"
+// columns; each thread owns two pairs sharing its "+" column (two independent fma
+// chains); row chunks of the 48 columns stream into a double buffer in shared
+// memory with cp.async while the previous chunk is consumed.
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem)
+{
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+// the 2x2 part of DMAGF2H for one pair: returns true when the pair needs the column
+// scan (then d holds the two leading terms of ABODNDF2 and t its coefficients)
+__device__ __forceinline__ bool hyp_pair_setup(const double *__restrict__ A, int n, int a, int b, int &p, int &q, bool &a_is_p,
+                                               double &w, double &d, Rot &t)
+{
+  a_is_p = (a < b);
+  p = a_is_p ? a : b;
+  q = a_is_p ? b : a;
+  const double app = A[(long long)p * n + p], aqp = A[(long long)p * n + q], apq = A[(long long)q * n + p], aqq = A[(long long)q * n + q];
+  w = nan_w();
+  if (!may_transform(app, aqp, apq, aqq)) return false;
+  double A2[4] = { app, aqp, apq, aqq }, U2[4], Z2[4];
+  int info = 0;
+  const int jp = a_is_p ? 1 : -1;  // "+" column a, "-" column b
+  dhsvd2(A2, jp, -jp, U2, Z2, JK_TH1FIX, info);
+  if (info < 0) return false;
+  if (!(info & 1)) { w = 0.0; return false; }
+  if (!(info & 4)) { w = dasum2(aqp, apq); return false; }
+  const double a1 = (info & 8) ? A2[M21] : 0.0, a2 = (info & 8) ? A2[M12] : 0.0;
+  d = 0.0;
+  d = fma(__dsub_rn(aqp, a1), __dadd_rn(aqp, a1), d);
+  d = fma(__dsub_rn(apq, a2), __dadd_rn(apq, a2), d);
+  t = rot_ab(Z2);
+  return true;
+}
+
+// The real hyperbolic weights in two kernels.  k_hyp_setup (one thread per pair)
+// runs the 2x2 HSVD of DMAGF2H and either writes the weight (no scan needed) or the
+// scan parameters of the pair; k_hyp_scan streams row chunks of 16 "+" x 16 PPT "-"
+// columns through a double buffer in shared memory (cp.async) and runs the
+// sequential ABODNDF2 fma chains, PPT pairs per thread sharing its "+" column.
+// Index-range tiles: tile (tp, tq), tp <= tq, holds the pairs p in [32 tp, 32 tp + 32),
+// q in [32 tq, 32 tq + 32), p < q, J(p) != J(q).  k_hyp_tile lists a tile's pairs,
+// runs their 2x2 HSVDs and either stores the weight (no scan) or the scan
+// parameters, then stages the tile's two column ranges in row chunks and runs the
+// fma chains.  Rows p and q can only lie in the two ranges, so the chunks outside
+// them run without a per-row skip test.
+#define TW 32
+#define SCAN_ROWS 64
+#define SCAN_RS (SCAN_ROWS + 2)
+
+__device__ __forceinline__ void tile_of(int b, int T, int &tp, int &tq)
+{
+  // b enumerates the tiles row by row of the upper triangle
+  int r = 0;
+  while (b >= T - r) { b -= T - r; ++r; }
+  tp = r;
+  tq = r + b;
+}
+
+// K pairs per thread (slots t, t + 256, ...); FAST: no row of this chunk is a p or q
+template <int K, bool FAST>
+__device__ __forceinline__ void scan_chunk(const double *const *xs, const double *const *ys, const int *pl, const int *ql,
+                                           const int *fl, const double *r1, const double *r2, const double *m1,
+                                           const double *m2, double *d, int rows)
+{
+#pragma unroll 2
+  for (int r = 0; r < rows; r += 2) {
+    double2 xv[K], yv[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      xv[k] = *(const double2 *)(xs[k] + r);
+      yv[k] = *(const double2 *)(ys[k] + r);
+    }
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      if (h == 1 && r + 1 >= rows) break;
+#pragma unroll
+      for (int k = 0; k < K; ++k) {
+        const double x = h ? xv[k].y : xv[k].x, y = h ? yv[k].y : yv[k].x;
+        const double xx = __dmul_rn(fma(y, r1[k], x), m1[k]);
+        const double yy = __dmul_rn(fma(x, r2[k], y), m2[k]);
+        const double e1 = fma(__dsub_rn(x, xx), __dadd_rn(x, xx), d[k]);
+        const double e2 = fma(__dsub_rn(y, yy), __dadd_rn(y, yy), e1);
+        if (FAST) d[k] = e2;  // inactive slots accumulate garbage that is never stored
+        else d[k] = ((fl[k] & 1) && (r + h) != pl[k] && (r + h) != ql[k]) ? e2 : d[k];
+      }
+    }
+  }
+}
+
+#define SCAN_THREADS 256
+#define SCAN_STAGES 3
+
+// one tile: list its pairs and run their 2x2 HSVDs (k_hyp_setup's work, parameters
+// to this tile's slice of `par`), then stream the two column ranges through a
+// three-stage buffer and run the fma chains, up to 4 pairs per thread
+__global__ void __launch_bounds__(SCAN_THREADS, 2)
+k_hyp_tile(const State *st, const double *__restrict__ A, const int *__restrict__ J, int n, double *__restrict__ Wm,
+           HypPar *par)
+{
+  if (st->stop) return;
+  const int T = (n + TW - 1) / TW;
+  int tp, tq;
+  tile_of(blockIdx.x, T, tp, tq);
+  const int P0 = tp * TW, Q0 = tq * TW;
+  HypPar *tpar = par + (long long)blockIdx.x * (TW * TW);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  __shared__ int s_cnt, s_warp[SCAN_THREADS / 32];
+  if (tid == 0) s_cnt = 0;
+  __syncthreads();
+  for (int base = 0; base < TW * TW; base += SCAN_THREADS) {
+    const int l = base + tid;
+    const int p = P0 + l / TW, q = Q0 + l % TW;
+    const bool hyp = (p < n) && (q < n) && (p < q) && (J[p] != J[q]);
+    const unsigned m = __ballot_sync(0xFFFFFFFFu, hyp);
+    if (!lane) s_warp[warp] = __popc(m);
+    __syncthreads();
+    int off = s_cnt;
+    for (int w2 = 0; w2 < warp; ++w2) off += s_warp[w2];
+    const int slot = off + __popc(m & ((1u << lane) - 1u));
+    __syncthreads();
+    if (tid == 0) { int t = 0; for (int w2 = 0; w2 < SCAN_THREADS / 32; ++w2) t += s_warp[w2]; s_cnt += t; }
+    if (hyp) {
+      int pp, qq;
+      bool ap;
+      double w, d0 = 0.0;
+      Rot t;
+      const int a = (J[p] == 1) ? p : q, bcol = (J[p] == 1) ? q : p;  // the "+" column first
+      const bool sc = hyp_pair_setup(A, n, a, bcol, pp, qq, ap, w, d0, t);
+      HypPar h;
+      h.p = pp; h.q = qq; h.pad = 0;
+      h.flags = sc ? (1 | (t.c1 ? 2 : 0) | (t.c2 ? 4 : 0)) : 0;
+      h.r1 = sc ? t.r1 : 0.0; h.r2 = sc ? t.r2 : 0.0; h.m1 = sc ? t.m1 : 0.0; h.m2 = sc ? t.m2 : 0.0;
+      h.d = d0;
+      tpar[slot] = h;
+      if (!sc) {
+        if (w < -JK_HUGE) w = nan_w();
+        Wm[(long long)qq * n + pp] = w;
+        Wm[(long long)pp * n + qq] = w;
+      }
+    }
+    __syncthreads();
+  }
+  const int cnt = s_cnt;
+  if (!cnt) return;
+
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double *buf = (double *)smem_raw;  // [SCAN_STAGES][2 * TW][SCAN_RS]: columns P0.., then Q0..
+  constexpr int K = 4, STAGE = 2 * TW * SCAN_RS;
+  int pl[K], ql[K], fl[K];
+  double r1[K], r2[K], m1[K], m2[K], d[K];
+  int kw = 0;  // active slots of this warp (warp-uniform)
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    const int slot = tid + SCAN_THREADS * k;
+    fl[k] = 0; pl[k] = ql[k] = 0; r1[k] = r2[k] = m1[k] = m2[k] = d[k] = 0.0;
+    if (slot < cnt) {
+      const HypPar h = tpar[slot];
+      fl[k] = h.flags; pl[k] = h.p - P0; ql[k] = h.q - Q0; d[k] = h.d;
+      r1[k] = h.r1; r2[k] = h.r2; m1[k] = h.m1; m2[k] = h.m2;
+    }
+    if (SCAN_THREADS * k + 32 * warp < cnt) kw = k + 1;
+  }
+  int any = 0, fastv = 1;
+#pragma unroll
+  for (int k = 0; k < K; ++k)
+    if (fl[k] & 1) { any = 1; if ((fl[k] & 6) != 6) fastv = 0; }
+  if (!__syncthreads_or(any)) return;
+  const bool allfast = __syncthreads_and(fastv);
+  const int nchunk = (n + SCAN_ROWS - 1) / SCAN_ROWS;
+  // staging: this thread copies row (tid & 63) of columns (tid >> 6) + 4 j, j = 0..15
+  const int sr = tid & (SCAN_ROWS - 1), sc0 = tid >> 6;
+  auto stage = [&](int c) {
+    if (c < nchunk) {
+      double *dst = buf + (c % SCAN_STAGES) * STAGE;
+      const int i0 = c * SCAN_ROWS;
+      if (i0 + sr < n) {
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+          const int col = sc0 + 4 * j;
+          const int g = (col < TW) ? (P0 + col) : (Q0 + col - TW);
+          if (g < n) cp_async8(dst + col * SCAN_RS + sr, A + (long long)g * n + i0 + sr);
+        }
+      }
+    }
+    cp_async_commit();  // an empty group past the last chunk keeps the wait count uniform
+  };
+  stage(0);
+  stage(1);
+  for (int c = 0; c < nchunk; ++c) {
+    cp_async_wait<1>();  // chunk c has landed (chunk c + 1 may be in flight)
+    __syncthreads();     // ... for every thread; and everyone is done with chunk c - 1
+    stage(c + 2);        // into the buffer of chunk c - 1
+    const double *bb = buf + (c % SCAN_STAGES) * STAGE;
+    const int i0 = c * SCAN_ROWS, rows = min(SCAN_ROWS, n - i0);
+    const double *xs[K], *ys[K];
+    int pr[K], qr[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      xs[k] = bb + pl[k] * SCAN_RS;
+      ys[k] = bb + (TW + ql[k]) * SCAN_RS;
+      pr[k] = pl[k] + P0 - i0;  // p, q as rows of this chunk
+      qr[k] = ql[k] + Q0 - i0;
+    }
+    const bool touch = (i0 < P0 + TW && P0 < i0 + rows) || (i0 < Q0 + TW && Q0 < i0 + rows);
+    if (allfast) {
+      if (!touch) {
+        if (kw == 4) scan_chunk<4, true>(xs, ys, pr, qr, fl, r1, r2, m1, m2, d, rows);
+        else if (kw == 3) scan_chunk<3, true>(xs, ys, pr, qr, fl, r1, r2, m1, m2, d, rows);
+        else if (kw == 2) scan_chunk<2, true>(xs, ys, pr, qr, fl, r1, r2, m1, m2, d, rows);
+        else if (kw == 1) scan_chunk<1, true>(xs, ys, pr, qr, fl, r1, r2, m1, m2, d, rows);
+      }
+      else {
+        if (kw == 4) scan_chunk<4, false>(xs, ys, pr, qr, fl, r1, r2, m1, m2, d, rows);
+        else if (kw == 3) scan_chunk<3, false>(xs, ys, pr, qr, fl, r1, r2, m1, m2, d, rows);
+        else if (kw == 2) scan_chunk<2, false>(xs, ys, pr, qr, fl, r1, r2, m1, m2, d, rows);
+        else if (kw == 1) scan_chunk<1, false>(xs, ys, pr, qr, fl, r1, r2, m1, m2, d, rows);
+      }
+    }
+    else {
+#pragma unroll
+      for (int k = 0; k < K; ++k)
+        if (fl[k] & 1) {
+          Rot t;
+          t.c1 = (fl[k] >> 1) & 1; t.c2 = (fl[k] >> 2) & 1;
+          t.r1 = r1[k]; t.r2 = r2[k]; t.m1 = m1[k]; t.m2 = m2[k];
+          scan_rows_real(xs[k], ys[k], rows, i0, pl[k] + P0, ql[k] + Q0, t, d[k]);
+        }
+    }
+  }
+  cp_async_wait<0>();
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    if (!(fl[k] & 1)) continue;
+    const int p = pl[k] + P0, q = ql[k] + Q0;
+    double x = d[k];
+    if (x < -JK_HUGE) x = nan_w();
+    Wm[(long long)q * n + p] = x;
+    Wm[(long long)p * n + q] = x;
+  }
+}
+
 template <typename T, int HP, int HM>
 __global__ void __launch_bounds__(HP * HM)
 k_weights_hyp(const State *st, const T *__restrict__ A, const int *__restrict__ plus, const int *__restrict__ minus,
@@ -358,18 +609,16 @@ k_weights_hyp(const State *st, const T *__restrict__ A, const int *__restrict__ 
 // greedy matching, so the matched edges are ranked and the first N_2 kept, in rank
 // order (the STEP array).
 //
-// The matching is computed with the Suitor algorithm (Manne and Halappanavar,
-// IPDPS 2014), which yields exactly the greedy matching for a total order of the
-// edges: every vertex proposes to its best partner for which it beats that
-// partner's current suitor; a displaced suitor proposes again further down its
-// list.  k_colsort ranks every vertex's partners (one block per column of the
-// symmetric weight matrix, a bitonic sort in shared memory); k_suitor runs the
-// proposals, one thread per vertex, with atomicCAS on a (rank << 16 | suitor) word
-// per vertex and no barriers; k_select collects the mutual pairs.
+// The matching is built in rounds: every free vertex proposes to its best free
+// partner and mutual proposals are matched; the best remaining edge of both its
+// endpoints is always taken by the walk, so the rounds rebuild the walk's matching
+// without touching the record list.  k_colsort ranks every vertex's partners once
+// per step (one block per column of the symmetric weight matrix; a bitonic sort held
+// in registers, shuffles and shared memory), so a round only moves each free
+// vertex's list pointer past partners matched meanwhile (k_select, one block).
 // ---------------------------------------------------------------------------
-#define SEL_THREADS 512
-#define SORT_THREADS 512
-#define SUITOR_EMPTY 0xFFFFFFFFu
+#define SEL_THREADS 1024
+#define SORT_THREADS 256
 
 // order-preserving 64-bit key of a weight; 0 for NaN (no record); -0 == +0
 __device__ __forceinline__ unsigned long long wkey(double w)
@@ -419,106 +668,128 @@ __host__ __device__ __forceinline__ int pow2ceil(int x)
   return s;
 }
 
-// rank the partners of vertex x = blockIdx.x: list[x][r] = r-th best partner,
-// rank[x][u] = position of u in that list; also resets the vertex's suitor state
-__global__ void __launch_bounds__(SORT_THREADS)
-k_colsort(const State *st, const double *__restrict__ Wm, int n, unsigned short *list, unsigned short *rank, int *len,
-          int *ptr, unsigned *suitor)
+// list row stride: 8 entries (16 bytes) per vector load
+__host__ __device__ __forceinline__ int list_ld(int n) { return (n + 7) & ~7; }
+
+// rank the partners of vertex v = blockIdx.x: list[v][r] = r-th best partner,
+// rank[v][u] = position of u in that list, len[v] = number of partners.
+// One 64-bit key per partner: the top 48 bits of the weight key, then the 16-bit
+// tie code (band << 1 | (u > v)), which orders the partners of v as (band, p) do
+// and also names u.  Partners whose keys agree in the top 48 bits are re-ordered by
+// the full key afterwards.  E keys per thread in registers (position tid*E + e);
+// stages with partner distance < E run in registers, < 32E by warp shuffles, the
+// rest in shared memory.
+__device__ __forceinline__ unsigned long long ckey(double w, int u, int v)
 {
-  if (st->stop) return;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int s2 = pow2ceil(n);
-  unsigned long long *k = (unsigned long long *)smem_raw;
-  unsigned *t = (unsigned *)(k + s2);
-  int *ix = (int *)(t + s2);
-  const int x = blockIdx.x;
-  const double *col = Wm + (long long)x * n;
-  __shared__ int s_cnt;
-  if (threadIdx.x == 0) s_cnt = 0;
-  __syncthreads();
-  int valid = 0;
-  for (int u = threadIdx.x; u < s2; u += blockDim.x) {
-    unsigned long long kk = 0ULL;
-    if (u < n && u != x) kk = wkey(col[u]);
-    k[u] = kk;
-    t[u] = kk ? tkey(u, x) : 0u;
-    ix[u] = kk ? u : -1;
-    valid += kk ? 1 : 0;
-  }
-  atomicAdd(&s_cnt, valid);
-  __syncthreads();
-  const int cnt = s_cnt;
-  bitonic_desc(k, t, ix, s2);
-  unsigned short *lx = list + (long long)x * n;
-  unsigned short *rx = rank + (long long)x * n;
-  for (int r = threadIdx.x; r < cnt; r += blockDim.x) {
-    const int u = ix[r];
-    lx[r] = (unsigned short)u;
-    rx[u] = (unsigned short)r;
-  }
-  if (threadIdx.x == 0) {
-    len[x] = cnt;
-    ptr[x] = 0;
-    suitor[x] = SUITOR_EMPTY;
-  }
+  const unsigned long long k = wkey(w);
+  if (!k) return 0ULL;
+  const unsigned b = (unsigned)((u < v) ? (v - u) : (u - v));
+  return ((k >> 16) << 16) | (unsigned long long)((b << 1) | (u > v ? 1u : 0u));
 }
 
-// the proposals: one thread per vertex; a thread that displaces a suitor continues
-// with the displaced vertex.  Every proposal either moves a list pointer forward or
-// strictly improves a suitor's rank, so the work is bounded (guard: 4 n^2 steps).
-#define SUITOR_BATCH 4
-__global__ void __launch_bounds__(128)
-k_suitor(State *st, int n, const unsigned short *__restrict__ list, const unsigned short *__restrict__ rank,
-         const int *__restrict__ len, int *ptr, unsigned *suitor)
+__device__ __forceinline__ int ckey_u(unsigned long long c, int v)
+{
+  const int t = (int)(c & 0xFFFFu);
+  return (t & 1) ? v + (t >> 1) : v - (t >> 1);
+}
+
+template <int E>
+__global__ void __launch_bounds__(SORT_THREADS)
+k_colsort(const State *st, const double *__restrict__ Wm, int n, unsigned short *list, unsigned short *rank, int *len)
 {
   if (st->stop) return;
-  int cur = blockIdx.x * blockDim.x + threadIdx.x;
-  if (cur >= n) return;
-  long long guard = 4LL * n * n + 64;
-  while (cur >= 0) {
-    int p = ptr[cur];
-    const int L = len[cur];
-    const unsigned short *lc = list + (long long)cur * n;
-    int next = -1;
-    bool placed = false;
-    while (p < L && !placed) {
-      const int m = (L - p < SUITOR_BATCH) ? (L - p) : SUITOR_BATCH;
-      int xs[SUITOR_BATCH];
-      unsigned rk[SUITOR_BATCH], sw[SUITOR_BATCH];
+  __shared__ unsigned long long sk[SORT_THREADS * E];
+  __shared__ int s_cnt;
+  const int v = blockIdx.x, tid = threadIdx.x;
+  const int s2 = SORT_THREADS * E;
+  const double *col = Wm + (long long)v * n;
+  unsigned long long k[E];
+  int valid = 0;
 #pragma unroll
-      for (int i = 0; i < SUITOR_BATCH; ++i)
-        if (i < m) xs[i] = lc[p + i];
-#pragma unroll
-      for (int i = 0; i < SUITOR_BATCH; ++i)
-        if (i < m) {
-          rk[i] = rank[(long long)xs[i] * n + cur];
-          sw[i] = __ldcg(&suitor[xs[i]]);
-        }
-#pragma unroll
-      for (int i = 0; i < SUITOR_BATCH; ++i) {
-        if (i >= m || placed) continue;
-        unsigned old = sw[i];
-        while ((old >> 16) > rk[i]) {
-          if (--guard < 0) { atomicMin(&st->err, -40); return; }
-          ptr[cur] = p + i + 1;  // where a later search for cur resumes
-          __threadfence();
-          const unsigned prev = atomicCAS(&suitor[xs[i]], old, (rk[i] << 16) | (unsigned)cur);
-          if (prev == old) {
-            placed = true;
-            next = (old == SUITOR_EMPTY) ? -1 : (int)(old & 0xFFFFu);
-            break;
-          }
-          old = prev;
-        }
-        if (placed) p = p + i + 1;
-      }
-      if (!placed) p += m;
-      if (--guard < 0) { atomicMin(&st->err, -40); return; }
-    }
-    if (!placed) ptr[cur] = p;
-    __threadfence();
-    cur = next;
+  for (int e = 0; e < E; ++e) {
+    const int i = tid * E + e;
+    k[e] = (i < n && i != v) ? ckey(col[i], i, v) : 0ULL;
+    valid += k[e] ? 1 : 0;
   }
+  if (tid == 0) s_cnt = 0;
+  __syncthreads();
+  atomicAdd(&s_cnt, valid);
+  for (int kk = 2; kk <= s2; kk <<= 1) {
+    for (int j = kk >> 1; j >= E; j >>= 1) {
+      if (j < 32 * E) {
+        const int m = j / E;
+        const bool lower = ((tid & m) == 0);
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+          const unsigned long long ok = __shfl_xor_sync(0xFFFFFFFFu, k[e], m);
+          const bool desc = (((tid * E + e) & kk) == 0);
+          // the lower position of a descending pair keeps the larger key
+          const unsigned long long hi = (ok > k[e]) ? ok : k[e], lo = (ok > k[e]) ? k[e] : ok;
+          k[e] = (desc == lower) ? hi : lo;
+        }
+      }
+      else {
+        __syncthreads();
+#pragma unroll
+        for (int e = 0; e < E; ++e) sk[tid * E + e] = k[e];
+        __syncthreads();
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+          const int i = tid * E + e, l = i ^ j;
+          const unsigned long long ok = sk[l];
+          const bool desc = ((i & kk) == 0), lower = (i < l);
+          const unsigned long long hi = (ok > k[e]) ? ok : k[e], lo = (ok > k[e]) ? k[e] : ok;
+          k[e] = (desc == lower) ? hi : lo;
+        }
+      }
+    }
+#pragma unroll
+    for (int jj = E / 2; jj > 0; jj >>= 1) {
+      if (jj < kk) {
+#pragma unroll
+        for (int e = 0; e < E; ++e) {
+          const int f = e ^ jj;
+          if (f > e) {
+            const bool desc = (((tid * E + e) & kk) == 0);
+            if (desc == (k[f] > k[e])) { const unsigned long long a = k[e]; k[e] = k[f]; k[f] = a; }
+          }
+        }
+      }
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int e = 0; e < E; ++e) sk[tid * E + e] = k[e];
+  __syncthreads();
+  const int cnt = s_cnt;
+  // runs of keys equal in their top 48 bits: order them by the full record order
+  for (int r = tid; r < cnt; r += blockDim.x) {
+    const unsigned long long h = sk[r] >> 16;
+    if ((r > 0 && (sk[r - 1] >> 16) == h) || r + 1 >= cnt || (sk[r + 1] >> 16) != h) continue;
+    int e = r + 1;
+    while (e + 1 < cnt && (sk[e + 1] >> 16) == h) ++e;
+    for (int i = r + 1; i <= e; ++i) {
+      const unsigned long long x = sk[i];
+      const unsigned long long fx = wkey(col[ckey_u(x, v)]);
+      int j = i - 1;
+      while (j >= r) {
+        const unsigned long long fy = wkey(col[ckey_u(sk[j], v)]);
+        if (fy > fx || (fy == fx && (sk[j] & 0xFFFFu) > (x & 0xFFFFu))) break;
+        sk[j + 1] = sk[j];
+        --j;
+      }
+      sk[j + 1] = x;
+    }
+  }
+  __syncthreads();
+  unsigned short *lv = list + (long long)v * list_ld(n);
+  unsigned short *rv = rank + (long long)v * n;
+  for (int r = tid; r < cnt; r += blockDim.x) {
+    const int u = ckey_u(sk[r], v);
+    lv[r] = (unsigned short)u;
+    rv[u] = (unsigned short)r;
+  }
+  if (tid == 0) len[v] = cnt;
 }
 
 // the end of the previous step: SL := MIN(SL, NL) and the loop test
@@ -544,6 +815,7 @@ __device__ void end_of_step(State *st, const Piv<T> *piv, const int *J, Trace &t
     if (st->trace_steps < st->trace_cap_steps) {
       const int s = st->trace_steps++;
       tr.sl[s] = sl; tr.nl[s] = (err < 0) ? err : nl; tr.tw[s] = tw; tr.trig[s] = tg; tr.hyp[s] = hy;
+      tr.rounds[s] = st->rounds;
     }
     for (int i = 0; i < sl; ++i)
       if (st->trace_npiv < st->trace_cap_piv) tr.piv[st->trace_npiv++] = make_int2(piv[i].p, piv[i].q);
@@ -553,13 +825,13 @@ __device__ void end_of_step(State *st, const Piv<T> *piv, const int *J, Trace &t
   else st->steps += 1;
 }
 
-// one block: the matched pairs, their ranking, the first N_2 pivots, their 2x2 HSVDs (the
-// first loop of DSTEP_TRANSF, src/D/dstep.F90:301-326: INFO, NL, the BA coefficients
-// of V) and the columns outside the pivot set.  A == nullptr: selection only.
+// one block: the end of the previous step, the matching rounds, the ranking of the
+// matched pairs and the first N_2 of them (the pivots of this step, rank order),
+// and the columns outside the pivot set
 template <typename T>
 __global__ void __launch_bounds__(SEL_THREADS, 1)
-k_select(State *st, const double *__restrict__ Wm, const T *__restrict__ A, const int *__restrict__ J, int n, int n_2,
-         const unsigned *suitor, Piv<T> *piv, RowRot<T> *rr, int *unp, Trace tr, int quirk)
+k_select(State *st, const double *__restrict__ Wm, const int *__restrict__ J, int n, int n_2,
+         const unsigned short *__restrict__ list, const int *__restrict__ len, Piv<T> *piv, int *unp, Trace tr)
 {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int s2 = pow2ceil(n / 2 > 0 ? n / 2 : 1);
@@ -567,28 +839,96 @@ k_select(State *st, const double *__restrict__ Wm, const T *__restrict__ A, cons
   unsigned *stie = (unsigned *)(skey + s2);                   // [s2]
   int *sidx = (int *)(stie + s2);                             // [s2]
   int2 *pairs = (int2 *)(sidx + s2);                          // [n/2 + 1]
-  unsigned char *ms = (unsigned char *)(pairs + (n / 2 + 1)); // [n]
-  __shared__ int s_stop, s_cnt, s_nl, s_err, s_nunp;
+  uint4 *win = (uint4 *)(pairs + (n / 2 + 1) + ((n / 2 + 1) & 1)); // [n]: 8 list entries from wbase
+  int *best = (int *)(win + n);                               // [n]
+  int *ptr = best + n;                                        // [n]
+  int *wbase = ptr + n;                                       // [n]
+  unsigned char *ms = (unsigned char *)(wbase + n);           // [n]
+  __shared__ int s_stop, s_cnt, s_got, s_nunp, s_rounds;
 
-  const int tid = threadIdx.x, nth = blockDim.x;
+  const int tid = threadIdx.x, nth = blockDim.x, ld = list_ld(n);
   if (tid == 0) {
     end_of_step<T>(st, piv, J, tr);
     s_stop = st->stop;
-    s_cnt = 0; s_nl = 0; s_err = 0; s_nunp = 0;
+    s_cnt = 0; s_nunp = 0; s_rounds = 0;
   }
   __syncthreads();
   if (s_stop) return;
-  // the mutual suitor pairs are the matching
   for (int v = tid; v < n; v += nth) {
-    const unsigned a = suitor[v];
-    if (a == SUITOR_EMPTY) continue;
-    const int u = (int)(a & 0xFFFFu);
-    const unsigned b = suitor[u];
-    if (v < u && b != SUITOR_EMPTY && (int)(b & 0xFFFFu) == v) pairs[atomicAdd(&s_cnt, 1)] = make_int2(v, u);
+    ms[v] = 0;
+    ptr[v] = 0;
+    wbase[v] = 0;
+    win[v] = *(const uint4 *)(list + (long long)v * ld);
   }
   __syncthreads();
 
-  // rank the matched pairs: bitonic sort on (weight key, tie key), descending
+  for (int round = 0; round <= n / 2 + 1; ++round) {
+    // phase A: the best free partner, the first free entry of the ranked list; the
+    // 8 entries at wbase are kept in shared memory, later ones are loaded on demand
+    for (int v = tid; v < n; v += nth) {
+      if (ms[v]) continue;
+      int p = ptr[v];
+      const int L = len[v];
+      const unsigned short *row = list + (long long)v * ld;
+      int found = -1;
+      while (p < L && found < 0) {
+        const int a = p & ~7;
+        if (a == wbase[v]) {
+          const uint4 q4 = win[v];
+          const unsigned w4[4] = { q4.x, q4.y, q4.z, q4.w };
+#pragma unroll
+          for (int e = 0; e < 8; ++e) {
+            const int idx = a + e;
+            const int u = (int)((w4[e >> 1] >> ((e & 1) * 16)) & 0xFFFFu);
+            if (found < 0 && idx >= p && idx < L && !ms[u]) { found = u; p = idx; }
+          }
+          if (found < 0) p = a + 8;
+          continue;
+        }
+        // past the window: fetch the next 32 entries with four independent loads
+        uint4 g4[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+          if (a + 8 * j < L) g4[j] = *(const uint4 *)(row + a + 8 * j);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          if (found >= 0 || a + 8 * j >= L) continue;
+          const unsigned w4[4] = { g4[j].x, g4[j].y, g4[j].z, g4[j].w };
+#pragma unroll
+          for (int e = 0; e < 8; ++e) {
+            const int idx = a + 8 * j + e;
+            const int u = (int)((w4[e >> 1] >> ((e & 1) * 16)) & 0xFFFFu);
+            if (found < 0 && idx >= p && idx < L && !ms[u]) { found = u; p = idx; }
+          }
+          if (found >= 0) { win[v] = g4[j]; wbase[v] = a + 8 * j; }
+        }
+        if (found < 0) p = a + 32;
+      }
+      if (found < 0) p = L;
+      ptr[v] = p;
+      best[v] = found;
+    }
+    if (tid == 0) { s_got = 0; s_rounds = round + 1; }
+    __syncthreads();
+    // phase B: mutual proposals are matched; a vertex without a candidate retires
+    for (int v = tid; v < n; v += nth) {
+      if (ms[v]) continue;
+      const int u = best[v];
+      if (u < 0) { ms[v] = 2; continue; }
+      if (v < u && best[u] == v) {
+        ms[v] = 1;
+        ms[u] = 1;
+        pairs[atomicAdd(&s_cnt, 1)] = make_int2(v, u);
+        atomicAdd(&s_got, 1);
+      }
+    }
+    __syncthreads();
+    const int got = s_got;
+    __syncthreads();
+    if (!got) break;
+  }
+
+  // rank the matched pairs: (weight key, tie key), descending
   const int np = s_cnt;
   for (int i = tid; i < s2; i += nth) {
     if (i < np) {
@@ -610,68 +950,81 @@ k_select(State *st, const double *__restrict__ Wm, const T *__restrict__ A, cons
     const int2 pr = pairs[sidx[r]];
     ms[pr.x] = 1;
     ms[pr.y] = 1;
-  }
-  __syncthreads();
-  for (int v = tid; v < n; v += nth)
-    if (!ms[v]) unp[atomicAdd(&s_nunp, 1)] = v;
-
-  for (int r = tid; r < sl; r += nth) {
-    const int2 pr = pairs[sidx[r]];
     Piv<T> &pv = piv[r];
     pv.p = pr.x;
     pv.q = pr.y;
     pv.w = Wm[(long long)pr.x * n + pr.y];
-    if (!A) continue;
-    const int p = pr.x, q = pr.y;
-    T B[4] = { A[(long long)p * n + p], A[(long long)p * n + q], A[(long long)q * n + p], A[(long long)q * n + q] };
-    T V[4], W[4];
-    int info = 0;
-    Tr<T>::hsvd2(B, J[p], J[q], V, W, JK_TH1FIX, info);
-    pv.info = info;
-    RowRot<T> x;
-    x.p = p; x.q = q; x.flags = 0;
-    if (info >= 0) {
-#pragma unroll
-      for (int k = 0; k < 4; ++k) { pv.V[k] = V[k]; pv.W[k] = W[k]; }
-      pv.d[0] = Tr<T>::re(B[M11]);
-      pv.d[1] = Tr<T>::re(B[M22]);
-      if (info & 2) {
-        const typename Tr<T>::R t = Tr<T>::ba(V, quirk);
-        x.flags = (t.c1 ? 1 : 0) | (t.c2 ? 2 : 0) | 4;
-        x.r1 = t.r1; x.r2 = t.r2; x.m1 = t.m1; x.m2 = t.m2;
-      }
-      if ((info & 1) && (info & 6)) atomicAdd(&s_nl, 1);
-    }
-    else
-      atomicMin(&s_err, info);
-    rr[r] = x;
   }
+  __syncthreads();
+  for (int v = tid; v < n; v += nth)
+    if (!ms[v]) unp[atomicAdd(&s_nunp, 1)] = v;
   __syncthreads();
   if (tid == 0) {
     st->sl = sl;
-    st->nl = s_nl;
-    st->err = s_err;
+    st->nl = 0;
+    st->err = 0;
     st->nunp = s_nunp;
+    st->rounds = s_rounds;
     if (sl <= 0) {
       // DSTEP_EXEC returns with SL = 0: the loop ends with INFO = S (src/D/dstep.F90:421, 575-582)
       st->info = st->steps;
       st->stop = 1;
       if (st->trace_on && st->trace_steps < st->trace_cap_steps) {
         const int s = st->trace_steps++;
-        tr.sl[s] = 0; tr.nl[s] = -1; tr.tw[s] = -0.0; tr.trig[s] = 0; tr.hyp[s] = 0;
+        tr.sl[s] = 0; tr.nl[s] = -1; tr.tw[s] = -0.0; tr.trig[s] = 0; tr.hyp[s] = 0; tr.rounds[s] = s_rounds;
       }
     }
     else st->pending = 1;
   }
 }
 
+// per pivot: the 2x2 HSVD of DSTEP_TRANSF's first loop (src/D/dstep.F90:301-326),
+// INFO, NL (src/D/dstep.F90:337) and the BA coefficients every rotating block reads
+template <typename T>
+__global__ void k_pivots(State *st, const T *__restrict__ A, const int *__restrict__ J, int n, Piv<T> *piv, RowRot<T> *rr, int quirk)
+{
+  if (st->stop) return;
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= st->sl) return;
+  Piv<T> &pv = piv[r];
+  const int p = pv.p, q = pv.q;
+  T B[4] = { A[(long long)p * n + p], A[(long long)p * n + q], A[(long long)q * n + p], A[(long long)q * n + q] };
+  T V[4], W[4];
+  int info = 0;
+  Tr<T>::hsvd2(B, J[p], J[q], V, W, JK_TH1FIX, info);
+  pv.info = info;
+  RowRot<T> x;
+  x.p = p; x.q = q; x.flags = 0;
+  if (info >= 0) {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) { pv.V[k] = V[k]; pv.W[k] = W[k]; }
+    pv.d[0] = Tr<T>::re(B[M11]);
+    pv.d[1] = Tr<T>::re(B[M22]);
+    if (info & 2) {
+      const typename Tr<T>::R t = Tr<T>::ba(V, quirk);
+      x.flags = (t.c1 ? 1 : 0) | (t.c2 ? 2 : 0) | 4;
+      x.r1 = t.r1; x.r2 = t.r2; x.m1 = t.m1; x.m2 = t.m2;
+    }
+    if ((info & 1) && (info & 6)) atomicAdd(&st->nl, 1);
+  }
+  else
+    atomicMin(&st->err, info);
+  rr[r] = x;
+}
+
 size_t select_smem(int n)
 {
   const int s2 = pow2ceil(n / 2 > 0 ? n / 2 : 1);
-  return (size_t)s2 * (8 + 4 + 4) + (size_t)(n / 2 + 1) * 8 + (size_t)n + 16;
+  const int np = (n / 2 + 1) + ((n / 2 + 1) & 1);
+  return (size_t)s2 * (8 + 4 + 4) + (size_t)np * 8 + (size_t)n * (16 + 4 + 4 + 4 + 1) + 16;
 }
 
-size_t colsort_smem(int n) { return (size_t)pow2ceil(n) * (8 + 4 + 4); }
+// k_colsort instantiations: records per thread E = pow2ceil(n) / SORT_THREADS
+int colsort_e(int n)
+{
+  const int s2 = pow2ceil(n);
+  return s2 <= SORT_THREADS ? 1 : s2 / SORT_THREADS;
+}
 // ---------------------------------------------------------------------------
 // the fused transformations of one step (src/D/dstep.F90:301-346).
 // Block b < SL owns pivot b's column pair (p, q); the other blocks own two
@@ -800,9 +1153,10 @@ cudaError_t prepare_kernels(int n)
   // dynamic shared memory beyond the default 48 KB: two columns of A per k_rotate
   // block, the ranking and matching state of k_select
   cudaError_t e = cudaFuncSetAttribute(k_rotate<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * n * 8);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_hyp_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, SCAN_STAGES * (2 * TW) * SCAN_RS * (int)sizeof(double));
   if (e == cudaSuccess) e = cudaFuncSetAttribute(k_rotate<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * n * 16);
   const int ss = (int)select_smem(n);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_colsort, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)colsort_smem(n));
   if (e == cudaSuccess) e = cudaFuncSetAttribute(k_select<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, ss);
   if (e == cudaSuccess) e = cudaFuncSetAttribute(k_select<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, ss);
   return e;
@@ -821,6 +1175,13 @@ cudaError_t launch_init(Workspace &w, void *U, void *Z, cudaStream_t s)
   return w.cplx ? init_t(w, (double2 *)U, (double2 *)Z, s) : init_t(w, (double *)U, (double *)Z, s);
 }
 
+static void hyp_d_launch(Workspace &w, const double *A, cudaStream_t s)
+{
+  const int T = (w.n + TW - 1) / TW, nt = T * (T + 1) / 2;
+  const size_t smem = SCAN_STAGES * (2 * TW) * SCAN_RS * sizeof(double);
+  k_hyp_tile<<<nt, SCAN_THREADS, smem, s>>>(w.st, A, w.J, w.n, w.Wm, (HypPar *)w.hpar);
+}
+
 template <typename T>
 static cudaError_t weights_t(Workspace &w, const T *A, cudaStream_t s)
 {
@@ -828,8 +1189,11 @@ static cudaError_t weights_t(Workspace &w, const T *A, cudaStream_t s)
   dim3 bt(32, 8), gt((n + 31) / 32, (n + 7) / 8);
   k_weights_trig<T><<<gt, bt, 0, s>>>(w.st, A, w.J, w.Wm, n);
   if (w.n_plus > 0 && w.n_minus > 0) {
-    // 16 x 16 pair tiles once they fill the GPU, 8 x 8 below
-    if ((long long)w.n_plus * w.n_minus >= 256LL * 148 * 4) {
+    // the pipelined real kernel once its tiles fill the GPU; 16 x 16 / 8 x 8 tiles otherwise
+    if (sizeof(T) == sizeof(double) && (long long)w.n_plus * w.n_minus >= 512LL * 148 * 2) {
+      hyp_d_launch(w, (const double *)A, s);
+    }
+    else if ((long long)w.n_plus * w.n_minus >= 256LL * 148 * 4) {
       dim3 gh((w.n_plus + 15) / 16, (w.n_minus + 15) / 16);
       k_weights_hyp<T, 16, 16><<<gh, 256, 0, s>>>(w.st, A, w.plus, w.minus, w.n_plus, w.n_minus, w.Wm, n);
     }
@@ -846,14 +1210,31 @@ cudaError_t launch_weights(Workspace &w, const void *A, cudaStream_t s)
   return w.cplx ? weights_t(w, (const double2 *)A, s) : weights_t(w, (const double *)A, s);
 }
 
+static cudaError_t colsort(Workspace &w, cudaStream_t s)
+{
+  const int n = w.n;
+  switch (colsort_e(n)) {
+  case 1: k_colsort<1><<<n, SORT_THREADS, 0, s>>>(w.st, w.Wm, n, w.list, w.rank, w.len); break;
+  case 2: k_colsort<2><<<n, SORT_THREADS, 0, s>>>(w.st, w.Wm, n, w.list, w.rank, w.len); break;
+  case 4: k_colsort<4><<<n, SORT_THREADS, 0, s>>>(w.st, w.Wm, n, w.list, w.rank, w.len); break;
+  case 8: k_colsort<8><<<n, SORT_THREADS, 0, s>>>(w.st, w.Wm, n, w.list, w.rank, w.len); break;
+  case 16: k_colsort<16><<<n, SORT_THREADS, 0, s>>>(w.st, w.Wm, n, w.list, w.rank, w.len); break;
+  default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
 template <typename T>
 static cudaError_t select_t(Workspace &w, const T *A, int n_2, cudaStream_t s)
 {
   const int n = w.n;
-  k_colsort<<<n, SORT_THREADS, colsort_smem(n), s>>>(w.st, w.Wm, n, w.list, w.rank, w.len, w.ptr, w.suitor);
-  k_suitor<<<(n + 127) / 128, 128, 0, s>>>(w.st, n, w.list, w.rank, w.len, w.ptr, w.suitor);
-  k_select<T><<<1, SEL_THREADS, select_smem(n), s>>>(w.st, w.Wm, A, w.J, n, n_2, w.suitor, (Piv<T> *)w.piv,
-                                                     (RowRot<T> *)w.rowrot, w.unp, w.tr, w.zba_quirk);
+  cudaError_t e = colsort(w, s);
+  if (e != cudaSuccess) return e;
+  k_select<T><<<1, SEL_THREADS, select_smem(n), s>>>(w.st, w.Wm, w.J, n, n_2, w.list, w.len, (Piv<T> *)w.piv, w.unp, w.tr);
+  if (A) {
+    const int half = n / 2 > 0 ? n / 2 : 1;
+    k_pivots<T><<<(half + 127) / 128, 128, 0, s>>>(w.st, A, w.J, n, (Piv<T> *)w.piv, (RowRot<T> *)w.rowrot, w.zba_quirk);
+  }
   return cudaGetLastError();
 }
 
@@ -893,6 +1274,48 @@ static cudaError_t finish_t(Workspace &w, T *A, T *Z, double *sigma, cudaStream_
 cudaError_t launch_finish(Workspace &w, void *A, void *Z, double *sigma, cudaStream_t s)
 {
   return w.cplx ? finish_t(w, (double2 *)A, (double2 *)Z, sigma, s) : finish_t(w, (double *)A, (double *)Z, sigma, s);
+}
+
+// FP64 FMA throughput probe: 8 independent dependent chains per thread
+__global__ void k_fp64_peak(double *out, int reps)
+{
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  double x0 = 1.0 + t * 1e-12, x1 = x0 + 1, x2 = x0 + 2, x3 = x0 + 3, x4 = x0 + 4, x5 = x0 + 5, x6 = x0 + 6, x7 = x0 + 7;
+  const double b = 0.999999, c = 1e-9;
+  for (int r = 0; r < reps; ++r) {
+    x0 = fma(x0, b, c); x1 = fma(x1, b, c); x2 = fma(x2, b, c); x3 = fma(x3, b, c);
+    x4 = fma(x4, b, c); x5 = fma(x5, b, c); x6 = fma(x6, b, c); x7 = fma(x7, b, c);
+  }
+  out[t] = x0 + x1 + x2 + x3 + x4 + x5 + x6 + x7;
+}
+
+double fp64_peak()
+{
+  int dev = 0, nsm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  const int blocks = nsm * 16, threads = 256, reps = 4000;
+  double *out = nullptr;
+  if (cudaMalloc(&out, (size_t)blocks * threads * sizeof(double)) != cudaSuccess) { cudaGetLastError(); return -1.0; }
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  k_fp64_peak<<<blocks, threads>>>(out, 100);
+  float best = 1e30f;
+  for (int it = 0; it < 3; ++it) {
+    cudaEventRecord(e0);
+    k_fp64_peak<<<blocks, threads>>>(out, reps);
+    cudaEventRecord(e1);
+    cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (ms < best) best = ms;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(out);
+  if (cudaGetLastError() != cudaSuccess) return -1.0;
+  return 2.0 * 8.0 * reps * (double)blocks * threads / (best * 1e-3) / 1e12;
 }
 
 cudaError_t launch_hsvd2_batch(int cplx, int count, void *A, const int *J, void *U, void *Z, int *info, double th1, cudaStream_t s)

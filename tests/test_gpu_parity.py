@@ -204,3 +204,17 @@ def test_device_pointer_entry():
     o = oracle.step_loop(Y, J, nt=1)
     assert info == o["info"]
     assert _same(U.cpu().numpy(), o["U"]) and _same(s.cpu().numpy(), o["sigma"])
+
+
+@pytest.mark.parametrize("graded", [False, True])
+def test_weights_bitexact_large_tiles(graded):
+    """Orders large enough for the two-kernel real hyperbolic path (setup + pipelined scan)."""
+    jk = _jk()
+    n = 800
+    Y, J = gen.graded(n, 1e-6, seed=21) if graded else gen.gaussian(n, seed=21, n_plus=400)
+    W = jk.weights(Y, J)
+    w, P, Q, tt = oracle.weights(Y, J, id_tru=1, nt=8)
+    got = W[P - 1, Q - 1]
+    assert _same(np.isnan(got), np.isnan(w))
+    m = ~np.isnan(w)
+    assert _same(got[m], w[m])
