@@ -58,6 +58,7 @@ typedef struct {
 #define JK_ERR_J (-23)          /* a J entry is not +1 or -1 (TRU1/TRU2, src/shared/jstep.F90:38-39) */
 #define JK_ERR_MAX_STEPS (-24)  /* opts->max_steps reached */
 #define JK_ERR_NO_DEVICE (-33)  /* no CUDA device */
+#define JK_ERR_SCRATCH (-34)    /* N beyond JK_NOALLOC_MAX_N (jk_dweights_noalloc) */
 
 /* DSTEP_LOOP with host buffers, src/D/dstep.F90:472-604 (copies to and from the device).
  * A is in/out; U, Z, SIGMA are out.  N_2 is clamped as JSTEP_LEN does (src/shared/jstep.F90:124). */
@@ -103,6 +104,23 @@ void jk_handle_destroy(jk_handle *h);
  * (leading dimension n) on `stream`; when dW is not NULL, also copy the symmetric
  * n x n weight matrix there (device pointer).  Returns 0 or an INFO error. */
 int jk_handle_weights(jk_handle *h, const double *dA, double *dW, void *stream);
+
+/* The pair weights of jk_handle_weights with no device allocation at all; no counterpart
+ * in the reference.  For callers that may not allocate where they need the weights:
+ * cudaMalloc/cudaFree synchronise the whole device (stalling the caller's other streams
+ * in a latency-bound loop) and fail once the device memory belongs to the caller's own
+ * pool.  dA (leading dimension n) and dW (n x n, only off-diagonal entries written) are
+ * device pointers, J the host sign vector, stream a cudaStream_t (NULL = default).
+ * Scratch (the stop flag, J and the +/- index lists) is a static device array for
+ * N <= JK_NOALLOC_MAX_N; larger N returns JK_ERR_SCRATCH.  The first call on each
+ * device looks up the array's device address (cudaGetSymbolAddress) and should come
+ * before any stream capture on that device.  All calls on a device share the array, so
+ * calls whose kernels may overlap (unordered streams) race: order them.  J is staged
+ * through a pageable copy, so the call returns before the kernels finish.
+ * Returns 0, -1 (N < 3), -2 (dA NULL), -4 (dW NULL), -8 (J NULL), JK_ERR_J,
+ * JK_ERR_SCRATCH or a CUDA error. */
+#define JK_NOALLOC_MAX_N 1024
+int jk_dweights_noalloc(int n, const double *dA, const int *J, double *dW, void *stream);
 
 /* Kernel launches enqueued by the calling thread's last step-loop call. */
 long long jk_last_launch_count(void);

@@ -22,7 +22,8 @@ import os
 import numpy as np
 
 __all__ = ["lib", "step_loop", "dstep_loop", "zstep_loop", "step_loop_dev", "hsvd2_batch", "weights", "select",
-           "read_yj", "write_uzs", "JkError", "jstep_len", "SYMBOLS"]
+           "read_yj", "write_uzs", "JkError", "jstep_len", "SYMBOLS", "weights_noalloc",
+           "NOALLOC_MAX_N"]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "_lib", "libjkogb_b200.so")
@@ -30,7 +31,7 @@ LIB_PATH = os.path.join(_HERE, "_lib", "libjkogb_b200.so")
 # every symbol include/jkogb.h declares
 SYMBOLS = ("jk_dstep_loop", "jk_zstep_loop", "jk_dstep_loop_dev", "jk_zstep_loop_dev", "jk_dhsvd2_batch",
            "jk_zhsvd2_batch", "jk_dweights", "jk_zweights", "jk_select", "jk_handle_create", "jk_handle_destroy",
-           "jk_handle_weights", "jk_last_launch_count", "jk_fp64_peak", "jk_max_order", "jk_strerror")
+           "jk_handle_weights", "jk_dweights_noalloc", "jk_last_launch_count", "jk_fp64_peak", "jk_max_order", "jk_strerror")
 
 
 class JkError(RuntimeError):
@@ -89,6 +90,8 @@ def lib():
         L.jk_handle_destroy.argtypes = [C.c_void_p]
         L.jk_handle_weights.restype = C.c_int
         L.jk_handle_weights.argtypes = [C.c_void_p, vp, vp, vp]
+        L.jk_dweights_noalloc.restype = C.c_int
+        L.jk_dweights_noalloc.argtypes = [C.c_int, vp, ip, vp, vp]
         L.jk_last_launch_count.restype = C.c_longlong
         L.jk_last_launch_count.argtypes = []
         L.jk_fp64_peak.restype = C.c_double
@@ -260,6 +263,22 @@ class Handle:
             self.close()
         except Exception:
             pass
+
+
+NOALLOC_MAX_N = 1024  # JK_NOALLOC_MAX_N
+
+
+def weights_noalloc(n, dA_ptr, J, dW_ptr, stream=0):
+    """jk_dweights_noalloc: the weights of the real device matrix at dA_ptr (n x n, column-major)
+    into the device matrix at dW_ptr (off-diagonal entries), enqueued on `stream` (a raw
+    cudaStream_t), with no device allocation; all calls on a device share one static scratch."""
+    Jc = np.ascontiguousarray(np.asarray(J, np.int32))
+    if Jc.shape != (int(n),):
+        raise ValueError("J must hold n signs")
+    rc = lib().jk_dweights_noalloc(int(n), C.c_void_p(dA_ptr), Jc.ctypes.data_as(C.POINTER(C.c_int)),
+                                   C.c_void_p(dW_ptr), C.c_void_p(stream))
+    if rc < 0:
+        raise JkError(rc, "weights_noalloc: ")
 
 
 def select(W, n_2):

@@ -403,6 +403,23 @@ int jk_handle_weights(jk_handle *h, const double *dA, double *dW, void *stream)
   return 0;
 }
 
+// Weights with no device allocation; scratch in a static device array (jk_kernels.cu).
+int jk_dweights_noalloc(int n, const double *dA, const int *J, double *dW, void *stream)
+{
+  static_assert(JK_NOALLOC_MAX_N == kNoallocMaxN, "header and library disagree on the scratch size");
+  if (n < 3) return -1;
+  if (n > JK_NOALLOC_MAX_N) return JK_ERR_SCRATCH;
+  if (!dA) return -2;
+  if (!J) return -8;
+  if (!dW) return -4;
+  for (int i = 0; i < n; ++i)
+    if (J[i] != 1 && J[i] != -1) return JK_ERR_J;
+  int rc = pick_device(nullptr);
+  if (rc) return rc;
+  CK(launch_weights_noalloc(n, dA, J, dW, (cudaStream_t)stream));
+  return 0;
+}
+
 long long jk_last_launch_count(void) { return g_launches; }
 
 double jk_fp64_peak(void)
@@ -433,6 +450,7 @@ const char *jk_strerror(int info)
   case JK_ERR_NOMEM: return "device memory allocation failed";
   case JK_ERR_TOO_LARGE: return "N too large for this build";
   case JK_ERR_NO_DEVICE: return "no CUDA device";
+  case JK_ERR_SCRATCH: return "N beyond the static scratch of jk_dweights_noalloc (JK_NOALLOC_MAX_N = 1024)";
   default: return "a 2x2 HSVD error (NaN or infinity in a pivot block) or argument error";
   }
 }

@@ -89,6 +89,9 @@ cudaError_t launch_weights(Workspace &w, const void *A, cudaStream_t s);
 cudaError_t launch_match(Workspace &w, int n_2, cudaStream_t s);
 cudaError_t launch_hsvd2_batch(int cplx, int count, void *A, const int *J, void *U, void *Z, int *info, double th1, cudaStream_t s);
 cudaError_t prepare_kernels(int n);
+// weights of a real matrix with no allocation: scratch in a static device array
+constexpr int kNoallocMaxN = 1024;
+cudaError_t launch_weights_noalloc(int n, const double *A, const int *J, double *W, cudaStream_t s);
 double fp64_peak();
 // kernel launches of one step (the graph body)
 constexpr int kStepLaunches = 6;

@@ -20,6 +20,8 @@
 #include <cooperative_groups.h>
 
 #include <cstdlib>
+#include <cstring>
+#include <mutex>
 
 #include "jk_internal.h"
 #include "jk_math.cuh"
@@ -1323,6 +1325,93 @@ cudaError_t launch_hsvd2_batch(int cplx, int count, void *A, const int *J, void 
   if (count <= 0) return cudaSuccess;
   if (cplx) k_hsvd2_batch<double2><<<(count + 127) / 128, 128, 0, s>>>(count, (double2 *)A, J, (double2 *)U, (double2 *)Z, info, th1);
   else k_hsvd2_batch<double><<<(count + 127) / 128, 128, 0, s>>>(count, (double *)A, J, (double *)U, (double *)Z, info, th1);
+  return cudaGetLastError();
+}
+
+
+// ---------------------------------------------------------------------------
+// Pair weights with no allocation at all (jk_dweights_noalloc).  Some callers may
+// not allocate device memory at the point where they need the weights: cudaMalloc
+// and cudaFree synchronise the whole device, which stalls a caller's other streams
+// inside a latency-bound loop, and they fail outright for a caller whose device
+// memory has already been handed to its own pool allocator.  For them the only
+// state the two weight kernels need besides A and W (the stop flag, J and the
+// "+"/"-" index lists) lives in the file-scope array below, sized for N up to
+// kNoallocMaxN.  The pipelined tile kernel needs per-tile parameter storage that
+// grows with N^2, so this form always uses the 16 x 16 / 8 x 8 tile kernel, whose
+// results are the same bit for bit.
+//
+// The array is shared by every call on a device: two calls whose kernels overlap
+// (different streams with no ordering between them) overwrite each other's J and
+// index lists and race.  The State record must start at zero (stop == 0); every
+// call copies a zeroed record in together with J and the index lists.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr size_t kScratchState = 256;  // State, padded to the alignment of what follows
+static_assert(sizeof(State) <= kScratchState, "State does not fit its scratch slot");
+constexpr size_t kScratchBytes = kScratchState + 3 * (size_t)kNoallocMaxN * sizeof(int);
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_scratch_mu;
+void *g_scratch_addr[kMaxDevices];  // device address of g_noalloc_scratch, per device
+
+// Set-up, once per device, with that device current: the device address of the
+// array.  The first call on a device therefore makes this runtime call, and should
+// come before any stream capture on that device.
+cudaError_t scratch_address(int dev, unsigned char **out)
+{
+  if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lk(g_scratch_mu);
+  if (!g_scratch_addr[dev]) {
+    void *a = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&a, g_noalloc_scratch);
+    if (e != cudaSuccess) return e;
+    g_scratch_addr[dev] = a;
+  }
+  *out = (unsigned char *)g_scratch_addr[dev];
+  return cudaSuccess;
+}
+
+}  // namespace
+
+cudaError_t launch_weights_noalloc(int n, const double *A, const int *J, double *W, cudaStream_t s)
+{
+  if (n < 1 || n > kNoallocMaxN) return cudaErrorInvalidValue;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  unsigned char *d = nullptr;
+  if ((e = scratch_address(dev, &d)) != cudaSuccess) return e;
+  // the image of the scratch on the host stack: a zeroed State, J, then the indices
+  // with J = +1 and with J = -1 in ascending order
+  alignas(16) unsigned char h[kScratchBytes];
+  memset(h, 0, kScratchState);
+  int *hj = (int *)(h + kScratchState), *hp = hj + kNoallocMaxN, *hm = hp + kNoallocMaxN;
+  int np = 0, nm = 0;
+  for (int i = 0; i < n; ++i) {
+    hj[i] = J[i];
+    if (J[i] == 1) hp[np++] = i;
+    else hm[nm++] = i;
+  }
+  // pageable source: the call returns once the bytes are staged, so the stack image may go
+  if ((e = cudaMemcpyAsync(d, h, kScratchBytes, cudaMemcpyHostToDevice, s)) != cudaSuccess) return e;
+  const State *st = (const State *)d;
+  const int *dj = (const int *)(d + kScratchState), *dp = dj + kNoallocMaxN, *dm = dp + kNoallocMaxN;
+  dim3 bt(32, 8), gt((n + 31) / 32, (n + 7) / 8);
+  k_weights_trig<double><<<gt, bt, 0, s>>>(st, A, dj, W, n);
+  if (np > 0 && nm > 0) {
+    if ((long long)np * nm >= 256LL * 148 * 4) {
+      dim3 gh((np + 15) / 16, (nm + 15) / 16);
+      k_weights_hyp<double, 16, 16><<<gh, 256, 0, s>>>(st, A, dp, dm, np, nm, W, n);
+    }
+    else {
+      dim3 gh((np + 7) / 8, (nm + 7) / 8);
+      k_weights_hyp<double, 8, 8><<<gh, 64, 0, s>>>(st, A, dp, dm, np, nm, W, n);
+    }
+  }
   return cudaGetLastError();
 }
 

@@ -47,3 +47,21 @@ def test_argument_errors_without_gpu():
     assert L.jk_dstep_loop(n, d(A), n, d(A), n, d(A), n, Jp, d(A), 0, 0, 0, ctypes.byref(o), None) == -23
     assert jk.jstep_len(7, 0) == 3 and jk.jstep_len(7, 9) == 3 and jk.jstep_len(7, 2) == 2
     assert "J" in jk.strerror(-23)
+
+
+def test_noalloc_argument_errors_without_gpu():
+    # jk_dweights_noalloc rejects N beyond its static scratch before any CUDA call
+    import numpy as np
+    import jkogb_b200 as jk
+    L = jk.lib()
+    n = jk.NOALLOC_MAX_N + 1
+    J = np.ones(n, np.int32)
+    Jp = J.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+    assert L.jk_dweights_noalloc(n, 16, Jp, 16, None) == -34
+    assert "static scratch" in jk.strerror(-34)
+    assert L.jk_dweights_noalloc(2, 16, Jp, 16, None) == -1
+    assert L.jk_dweights_noalloc(8, None, Jp, 16, None) == -2
+    assert L.jk_dweights_noalloc(8, 16, None, 16, None) == -8
+    assert L.jk_dweights_noalloc(8, 16, Jp, None, None) == -4
+    J[3] = 0
+    assert L.jk_dweights_noalloc(8, 16, Jp, 16, None) == -23
