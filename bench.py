@@ -267,7 +267,8 @@ def run_ours(args, wl):
 
 def _recorded_traffic(workload):
     try:
-        return json.load(open(os.path.join(ROOT, "profiles", "traffic.json"))).get(workload)
+        rec = json.load(open(os.path.join(ROOT, "profiles", "traffic.json"))).get(workload)
+        return float(rec["bytes_per_launch"]) if rec else None
     except Exception:
         return None
 

@@ -1,0 +1,60 @@
+"""Run one named workload through the library on the current GPU.
+
+  python -m jkogb_b200.run WORKLOAD [--max-steps S] [--weights R]
+
+Without --weights: one device-resident solve of the workload (jk_dstep_loop_dev /
+jk_zstep_loop_dev), stopped after S steps when --max-steps is given (the API's own step
+limit, INFO = -24), and prints INFO and the wall time.  With --weights R: R launches of
+one build's pair weights (jk_handle_weights) on the workload's input Y, the kernel-level
+form of the weight phase.  Both are the small, bounded invocations a profiler is pointed at.
+"""
+from __future__ import annotations
+
+import argparse
+import time
+
+import numpy as np
+
+from . import gen
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(prog="python -m jkogb_b200.run")
+    ap.add_argument("workload", choices=sorted(gen.WORKLOADS))
+    ap.add_argument("--max-steps", type=int, default=0)
+    ap.add_argument("--weights", type=int, default=0)
+    a = ap.parse_args(argv)
+
+    import torch
+
+    import jkogb_b200 as jk
+
+    wl = gen.WORKLOADS[a.workload]
+    Y, J = wl["make"]()
+    n, n_2 = wl["n"], wl["n_2"]
+    cplx = wl["kind"] == "complex"
+    tdt = torch.complex128 if cplx else torch.float64
+    dev = torch.device("cuda", 0)
+    Y0 = torch.from_numpy(np.ascontiguousarray(Y.T)).to(dev).t()
+    stream = torch.cuda.current_stream(dev)
+    t0 = time.perf_counter()
+    if a.weights > 0:
+        h = jk.Handle(n, J, complex_=cplx)
+        for _ in range(a.weights):
+            h.weights(Y0.data_ptr(), None, stream.cuda_stream)
+        torch.cuda.synchronize(dev)
+        h.close()
+        print(f"{a.workload}: {a.weights} weight launches in {time.perf_counter() - t0:.3f} s")
+        return 0
+    A = Y0.clone().t().contiguous().t()
+    U = torch.empty((n, n), dtype=tdt, device=dev).t()
+    Z = torch.empty((n, n), dtype=tdt, device=dev).t()
+    s = torch.empty(n, dtype=torch.float64, device=dev)
+    info = jk.step_loop_dev(A, U, Z, s, J, n_2=n_2, stream=stream, max_steps=a.max_steps)
+    torch.cuda.synchronize(dev)
+    print(f"{a.workload}: INFO={info} in {time.perf_counter() - t0:.3f} s")
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())
