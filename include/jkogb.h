@@ -122,6 +122,30 @@ int jk_handle_weights(jk_handle *h, const double *dA, double *dW, void *stream);
 #define JK_NOALLOC_MAX_N 1024
 int jk_dweights_noalloc(int n, const double *dA, const int *J, double *dW, void *stream);
 
+/* Batched solve: `count` independent real matrices of orders n[m] (3 <= n[m] <=
+ * JK_BATCH_MAX_N), each through the whole DSTEP_LOOP (src/D/dstep.F90:472-604) with its
+ * own N_2 n_2[m] (clamped as JSTEP_LEN does), all in one persistent launch (one thread
+ * block per matrix at a time, largest matrices first).  Packed layout: matrix m's
+ * column-major n[m] x n[m] blocks of A, U, Z start at sum_{k<m} n[k]^2 doubles; its J
+ * and SIGMA entries at sum_{k<m} n[k].  info[m] is the matrix's INFO (>= 0 steps, < 0
+ * error).  Results equal jk_dstep_loop's on each matrix. */
+#define JK_BATCH_MAX_N 128
+typedef struct jk_batch jk_batch;
+/* A plan for one batch shape (orders, N_2, J: host arrays); opts: max_steps, device. */
+jk_batch *jk_batch_create(int count, const int *n, const int *n_2, const int *J, const jk_opts *opts, int *info);
+void jk_batch_destroy(jk_batch *b);
+/* Enqueue the solve on device buffers (packed as above) on `stream`; A in/out, U, Z,
+ * SIGMA, INFO out.  The launch is captured once per set of buffers as a CUDA graph
+ * and replayed.  Returns 0 or an error; does not synchronise. */
+int jk_batch_run(jk_batch *b, double *dA, double *dU, double *dZ, double *dsigma, int *dinfo, void *stream);
+/* Autotune the block shape (threads per block) on this batch: solves a copy of dA with
+ * every candidate, keeps the fastest for later runs and returns its thread count.  dA
+ * is left unchanged; dU, dZ, dsigma, dinfo receive a solve's outputs. */
+int jk_batch_tune(jk_batch *b, const double *dA, double *dU, double *dZ, double *dsigma, int *dinfo, void *stream);
+/* The same with host buffers (copies in and out, synchronous).  Returns 0 or an error. */
+int jk_dstep_loop_batched(int count, const int *n, const int *n_2, double *A, double *U, double *Z, const int *J,
+                          double *sigma, int *info, const jk_opts *opts);
+
 /* Kernel launches enqueued by the calling thread's last step-loop call. */
 long long jk_last_launch_count(void);
 

@@ -23,7 +23,7 @@ import numpy as np
 
 __all__ = ["lib", "step_loop", "dstep_loop", "zstep_loop", "step_loop_dev", "hsvd2_batch", "weights", "select",
            "read_yj", "write_uzs", "JkError", "jstep_len", "SYMBOLS", "weights_noalloc",
-           "NOALLOC_MAX_N"]
+           "NOALLOC_MAX_N", "dstep_loop_batched", "Batch", "batch_pack", "batch_unpack", "BATCH_MAX_N"]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "_lib", "libjkogb_b200.so")
@@ -31,7 +31,8 @@ LIB_PATH = os.path.join(_HERE, "_lib", "libjkogb_b200.so")
 # every symbol include/jkogb.h declares
 SYMBOLS = ("jk_dstep_loop", "jk_zstep_loop", "jk_dstep_loop_dev", "jk_zstep_loop_dev", "jk_dhsvd2_batch",
            "jk_zhsvd2_batch", "jk_dweights", "jk_zweights", "jk_select", "jk_handle_create", "jk_handle_destroy",
-           "jk_handle_weights", "jk_dweights_noalloc", "jk_last_launch_count", "jk_fp64_peak", "jk_max_order", "jk_strerror")
+           "jk_handle_weights", "jk_dweights_noalloc", "jk_batch_create", "jk_batch_destroy",
+           "jk_batch_run", "jk_batch_tune", "jk_dstep_loop_batched", "jk_last_launch_count", "jk_fp64_peak", "jk_max_order", "jk_strerror")
 
 
 class JkError(RuntimeError):
@@ -92,6 +93,16 @@ def lib():
         L.jk_handle_weights.argtypes = [C.c_void_p, vp, vp, vp]
         L.jk_dweights_noalloc.restype = C.c_int
         L.jk_dweights_noalloc.argtypes = [C.c_int, vp, ip, vp, vp]
+        L.jk_batch_create.restype = C.c_void_p
+        L.jk_batch_create.argtypes = [C.c_int, ip, ip, ip, C.POINTER(Opts), ip]
+        L.jk_batch_destroy.restype = None
+        L.jk_batch_destroy.argtypes = [C.c_void_p]
+        L.jk_batch_run.restype = C.c_int
+        L.jk_batch_run.argtypes = [C.c_void_p, vp, vp, vp, vp, vp, vp]
+        L.jk_batch_tune.restype = C.c_int
+        L.jk_batch_tune.argtypes = [C.c_void_p, vp, vp, vp, vp, vp, vp]
+        L.jk_dstep_loop_batched.restype = C.c_int
+        L.jk_dstep_loop_batched.argtypes = [C.c_int, ip, ip, vp, vp, vp, ip, vp, ip, C.POINTER(Opts)]
         L.jk_last_launch_count.restype = C.c_longlong
         L.jk_last_launch_count.argtypes = []
         L.jk_fp64_peak.restype = C.c_double
@@ -279,6 +290,87 @@ def weights_noalloc(n, dA_ptr, J, dW_ptr, stream=0):
                                    C.c_void_p(dW_ptr), C.c_void_p(stream))
     if rc < 0:
         raise JkError(rc, "weights_noalloc: ")
+
+
+BATCH_MAX_N = 128  # JK_BATCH_MAX_N
+
+
+def batch_pack(mats, Js):
+    """Pack real square matrices (column-major blocks, one after the other) and their sign
+    vectors the way the batched entry points expect; returns (A, J, n, offsets)."""
+    n = np.array([np.asarray(Y).shape[0] for Y in mats], np.int32)
+    off = np.concatenate([[0], np.cumsum(n.astype(np.int64) ** 2)])
+    A = np.empty(int(off[-1]), np.float64)
+    for m, Y in enumerate(mats):
+        A[off[m]:off[m + 1]] = np.asarray(Y, np.float64).ravel(order="F")
+    J = np.ascontiguousarray(np.concatenate([np.asarray(j) for j in Js]).astype(np.int32))
+    return A, J, n, off
+
+
+def batch_unpack(X, n, off):
+    """The column-major blocks of a packed batch as a list of n x n arrays."""
+    return [X[off[m]:off[m + 1]].reshape((n[m], n[m]), order="F") for m in range(len(n))]
+
+
+def dstep_loop_batched(mats, Js, n_2=None, max_steps=0):
+    """jk_dstep_loop_batched on host arrays: every matrix through the whole step loop in one
+    persistent launch.  n_2: per-matrix N_2 (default 0, i.e. N/2).  Returns a list of dicts
+    (info, A, U, Z, sigma) as dstep_loop returns them."""
+    A, J, n, off = batch_pack(mats, Js)
+    cnt = len(n)
+    n2 = np.ascontiguousarray(np.zeros(cnt, np.int32) if n_2 is None else np.asarray(n_2, np.int32))
+    U = np.empty_like(A)
+    Z = np.empty_like(A)
+    sig = np.empty(int(np.sum(n)), np.float64)
+    info = np.zeros(cnt, np.int32)
+    o = _opts(max_steps)
+    ip = lambda a: a.ctypes.data_as(C.POINTER(C.c_int))  # noqa: E731
+    rc = lib().jk_dstep_loop_batched(cnt, ip(n), ip(n2), A.ctypes.data, U.ctypes.data, Z.ctypes.data, ip(J),
+                                     sig.ctypes.data, ip(info), C.byref(o))
+    if rc < 0:
+        raise JkError(rc, "batched step loop: ")
+    so = np.concatenate([[0], np.cumsum(n)])
+    As, Us, Zs = batch_unpack(A, n, off), batch_unpack(U, n, off), batch_unpack(Z, n, off)
+    return [dict(info=int(info[m]), A=As[m], U=Us[m], Z=Zs[m], sigma=sig[so[m]:so[m + 1]]) for m in range(cnt)]
+
+
+class Batch:
+    """A plan of the batched solver for one batch shape (jk_batch_create); run() and tune()
+    take raw device pointers of the packed buffers (see batch_pack)."""
+
+    def __init__(self, n, n_2, J, max_steps=0):
+        self.n = np.ascontiguousarray(np.asarray(n, np.int32))
+        self.n_2 = np.ascontiguousarray(np.asarray(n_2, np.int32))
+        Jc = np.ascontiguousarray(np.asarray(J, np.int32))
+        info = C.c_int(0)
+        o = _opts(max_steps)
+        ip = lambda a: a.ctypes.data_as(C.POINTER(C.c_int))  # noqa: E731
+        self._b = lib().jk_batch_create(len(self.n), ip(self.n), ip(self.n_2), ip(Jc), C.byref(o), C.byref(info))
+        if not self._b:
+            raise JkError(info.value, "batch plan: ")
+
+    def run(self, dA, dU, dZ, dsigma, dinfo, stream=0):
+        rc = lib().jk_batch_run(self._b, dA, dU, dZ, dsigma, dinfo, C.c_void_p(stream))
+        if rc < 0:
+            raise JkError(rc, "batch run: ")
+
+    def tune(self, dA, dU, dZ, dsigma, dinfo, stream=0):
+        """Choose the block shape on this batch; returns the chosen threads per block."""
+        rc = lib().jk_batch_tune(self._b, dA, dU, dZ, dsigma, dinfo, C.c_void_p(stream))
+        if rc < 0:
+            raise JkError(rc, "batch tune: ")
+        return rc
+
+    def close(self):
+        if self._b:
+            lib().jk_batch_destroy(self._b)
+            self._b = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def select(W, n_2):

@@ -4,6 +4,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <algorithm>
 #include <vector>
 
 #include "../../include/jkogb.h"
@@ -418,6 +419,204 @@ int jk_dweights_noalloc(int n, const double *dA, const int *J, double *dW, void 
   if (rc) return rc;
   CK(launch_weights_noalloc(n, dA, J, dW, (cudaStream_t)stream));
   return 0;
+}
+
+// ---------------------------------------------------------------------------
+// the batched solver: many small real matrices, one persistent launch (jk_batch.cu)
+// ---------------------------------------------------------------------------
+struct jk_batch {
+  Guard g;
+  int count = 0, nm = 0, variant = kBatchVariants - 1, grid = 0;
+  long long cap = 0, total = 0, totaln = 0;
+  BatchItem *items = nullptr;
+  int *counter = nullptr, *J = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  const void *key[6] = {};  // the buffers and stream the graph was captured with
+  int key_variant = -1;
+  ~jk_batch()
+  {
+    if (exec) cudaGraphExecDestroy(exec);
+  }
+};
+
+static int batch_grid(int variant, int nm)
+{
+  int dev = 0, sms = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return sms * batch_blocks_per_sm(variant, nm);
+}
+
+jk_batch *jk_batch_create(int count, const int *n, const int *n_2, const int *J, const jk_opts *opts, int *info)
+{
+  int rc = 0;
+  if (count < 1) rc = -1;
+  else if (!n) rc = -2;
+  else if (!n_2) rc = -3;
+  else if (!J) rc = -4;
+  long long total = 0, totaln = 0;
+  int nm = 0;
+  for (int m = 0; !rc && m < count; ++m) {
+    if (n[m] < 3) rc = -2;
+    else if (n[m] > JK_BATCH_MAX_N) rc = JK_ERR_TOO_LARGE;
+    else if (n_2[m] < 0) rc = -3;
+    for (int i = 0; !rc && i < n[m]; ++i)
+      if (J[totaln + i] != 1 && J[totaln + i] != -1) rc = JK_ERR_J;
+    if (!rc) {
+      total += (long long)n[m] * n[m];
+      totaln += n[m];
+      nm = (n[m] > nm) ? n[m] : nm;
+    }
+  }
+  if (!rc) rc = pick_device(opts);
+  jk_batch *b = nullptr;
+  if (!rc) {
+    b = new jk_batch;
+    b->count = count;
+    b->nm = nm;
+    b->total = total;
+    b->totaln = totaln;
+    b->cap = (opts && opts->max_steps > 0) ? opts->max_steps : (4000LL * nm + 100000LL);
+    // the work order: largest matrices first (the cost grows as N^4)
+    std::vector<BatchItem> it(count);
+    long long off = 0;
+    int joff = 0;
+    for (int m = 0; m < count; ++m) {
+      it[m].off = off;
+      it[m].n = n[m];
+      it[m].n_2 = jstep_len(n[m], n_2[m]);
+      it[m].joff = joff;
+      it[m].index = m;
+      off += (long long)n[m] * n[m];
+      joff += n[m];
+    }
+    std::stable_sort(it.begin(), it.end(), [](const BatchItem &x, const BatchItem &y) { return x.n > y.n; });
+    auto fail = [&](cudaError_t e) { rc = cuda_fail(e); };
+    cudaError_t e = b->g.alloc(&b->items, count * sizeof(BatchItem));
+    if (e == cudaSuccess) e = b->g.alloc(&b->counter, sizeof(int));
+    if (e == cudaSuccess) e = b->g.alloc(&b->J, totaln * sizeof(int));
+    if (e == cudaSuccess) e = cudaMemcpy(b->items, it.data(), count * sizeof(BatchItem), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(b->J, J, totaln * sizeof(int), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = batch_prepare(nm);
+    if (e != cudaSuccess) fail(e);
+    if (!rc) {
+      b->grid = batch_grid(b->variant, nm);
+      if (b->grid <= 0) rc = JK_ERR_CUDA;
+    }
+    if (rc) { delete b; b = nullptr; }
+  }
+  if (info) *info = rc;
+  return b;
+}
+
+void jk_batch_destroy(jk_batch *b) { delete b; }
+
+int jk_batch_run(jk_batch *b, double *dA, double *dU, double *dZ, double *dsigma, int *dinfo, void *stream)
+{
+  if (!b || !dA || !dU || !dZ || !dsigma || !dinfo) return -1;
+  cudaStream_t s = (cudaStream_t)stream;
+  const void *key[6] = { dA, dU, dZ, dsigma, dinfo, stream };
+  bool same = (b->exec != nullptr) && (b->key_variant == b->variant);
+  for (int k = 0; k < 6; ++k) same = same && (key[k] == b->key[k]);
+  if (!same) {
+    if (b->exec) { cudaGraphExecDestroy(b->exec); b->exec = nullptr; }
+    // capture the launch (counter reset + persistent kernel) once per set of buffers
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+      const cudaError_t e1 = launch_batch(b->variant, b->grid, b->items, b->count, b->counter, dA, dU, dZ, b->J, dsigma,
+                                          dinfo, b->nm, b->cap, s);
+      const cudaError_t e2 = cudaStreamEndCapture(s, &graph);
+      e = (e1 != cudaSuccess) ? e1 : e2;
+    }
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&b->exec, graph, 0);
+    if (graph) cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      b->exec = nullptr;
+      g_launches = 1;
+      CK(launch_batch(b->variant, b->grid, b->items, b->count, b->counter, dA, dU, dZ, b->J, dsigma, dinfo, b->nm,
+                      b->cap, s));
+      return 0;
+    }
+    for (int k = 0; k < 6; ++k) b->key[k] = key[k];
+    b->key_variant = b->variant;
+  }
+  g_launches = 1;
+  CK(cudaGraphLaunch(b->exec, s));
+  return 0;
+}
+
+int jk_batch_tune(jk_batch *b, const double *dA, double *dU, double *dZ, double *dsigma, int *dinfo, void *stream)
+{
+  if (!b || !dA || !dU || !dZ || !dsigma || !dinfo) return -1;
+  cudaStream_t s = (cudaStream_t)stream;
+  Guard g;
+  double *scratch = nullptr;
+  CK(g.alloc(&scratch, b->total * sizeof(double)));
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  float best_ms = -1.0f;
+  int best = b->variant;
+  cudaError_t err = cudaSuccess;
+  for (int v = 0; v < kBatchVariants && err == cudaSuccess; ++v) {
+    const int grid = batch_grid(v, b->nm);
+    if (grid <= 0) continue;
+    err = cudaMemcpyAsync(scratch, dA, b->total * sizeof(double), cudaMemcpyDeviceToDevice, s);
+    if (err == cudaSuccess) err = cudaEventRecord(e0, s);
+    if (err == cudaSuccess)
+      err = launch_batch(v, grid, b->items, b->count, b->counter, scratch, dU, dZ, b->J, dsigma, dinfo, b->nm, b->cap, s);
+    if (err == cudaSuccess) err = cudaEventRecord(e1, s);
+    if (err == cudaSuccess) err = cudaEventSynchronize(e1);
+    float ms = 0.0f;
+    if (err == cudaSuccess) err = cudaEventElapsedTime(&ms, e0, e1);
+    if (err == cudaSuccess && (best_ms < 0.0f || ms < best_ms)) { best_ms = ms; best = v; }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (err != cudaSuccess) return cuda_fail(err);
+  b->variant = best;
+  b->grid = batch_grid(best, b->nm);
+  return kBatchThreads[best];
+}
+
+int jk_dstep_loop_batched(int count, const int *n, const int *n_2, double *A, double *U, double *Z, const int *J,
+                          double *sigma, int *info, const jk_opts *opts)
+{
+  if (!A || !U || !Z || !sigma || !info) return -5;
+  int rc = 0;
+  jk_batch *b = jk_batch_create(count, n, n_2, J, opts, &rc);
+  if (!b) return rc;
+  Guard g;
+  double *dA = nullptr, *dU = nullptr, *dZ = nullptr, *ds = nullptr;
+  int *di = nullptr;
+  cudaStream_t s = nullptr;
+  auto body = [&]() -> int {
+    CK(g.alloc(&dA, b->total * sizeof(double)));
+    CK(g.alloc(&dU, b->total * sizeof(double)));
+    CK(g.alloc(&dZ, b->total * sizeof(double)));
+    CK(g.alloc(&ds, b->totaln * sizeof(double)));
+    CK(g.alloc(&di, count * sizeof(int)));
+    CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    CK(cudaMemcpyAsync(dA, A, b->total * sizeof(double), cudaMemcpyHostToDevice, s));
+    const int r = jk_batch_run(b, dA, dU, dZ, ds, di, s);
+    if (r) return r;
+    CK(cudaMemcpyAsync(A, dA, b->total * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(U, dU, b->total * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(Z, dZ, b->total * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(sigma, ds, b->totaln * sizeof(double), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(info, di, count * sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    return 0;
+  };
+  rc = body();
+  if (b->exec) { cudaGraphExecDestroy(b->exec); b->exec = nullptr; }
+  if (s) cudaStreamDestroy(s);
+  jk_batch_destroy(b);
+  return rc;
 }
 
 long long jk_last_launch_count(void) { return g_launches; }

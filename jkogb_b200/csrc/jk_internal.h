@@ -89,6 +89,23 @@ cudaError_t launch_weights(Workspace &w, const void *A, cudaStream_t s);
 cudaError_t launch_match(Workspace &w, int n_2, cudaStream_t s);
 cudaError_t launch_hsvd2_batch(int cplx, int count, void *A, const int *J, void *U, void *Z, int *info, double th1, cudaStream_t s);
 cudaError_t prepare_kernels(int n);
+// the batched solver (jk_batch.cu): one matrix of the packed batch
+struct BatchItem {
+  long long off;  // offset of its n x n blocks in A, U, Z (doubles)
+  int n, n_2;     // order and N_2 (clamped as JSTEP_LEN does)
+  int joff;       // offset of its J and SIGMA entries
+  int index;      // position in the caller's batch (INFO slot)
+};
+constexpr int kBatchMaxN = 128;
+constexpr int kBatchVariants = 3;
+constexpr int kInfoMaxSteps = -24;
+extern const int kBatchThreads[kBatchVariants];
+size_t batch_smem(int nm);
+cudaError_t batch_prepare(int nm);
+int batch_blocks_per_sm(int variant, int nm);
+cudaError_t launch_batch(int variant, int grid, const BatchItem *items, int count, int *counter, double *A, double *U,
+                         double *Z, const int *J, double *sigma, int *info, int nm, long long cap, cudaStream_t s);
+
 // weights of a real matrix with no allocation: scratch in a static device array
 constexpr int kNoallocMaxN = 1024;
 cudaError_t launch_weights_noalloc(int n, const double *A, const int *J, double *W, cudaStream_t s);

@@ -65,3 +65,26 @@ def test_noalloc_argument_errors_without_gpu():
     assert L.jk_dweights_noalloc(8, 16, Jp, None, None) == -4
     J[3] = 0
     assert L.jk_dweights_noalloc(8, 16, Jp, 16, None) == -23
+
+
+def test_batched_argument_errors_without_gpu():
+    # the batched plan checks orders, N_2 and J before any CUDA call
+    import numpy as np
+    import jkogb_b200 as jk
+    L = jk.lib()
+    ip = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_int))  # noqa: E731
+    n = np.array([16, jk.BATCH_MAX_N + 2], np.int32)
+    n2 = np.zeros(2, np.int32)
+    J = np.ones(int(n.sum()), np.int32)
+    info = ctypes.c_int(0)
+    assert not L.jk_batch_create(2, ip(n), ip(n2), ip(J), None, ctypes.byref(info))
+    assert info.value == -32
+    n[1] = 2
+    assert not L.jk_batch_create(2, ip(n), ip(n2), ip(J), None, ctypes.byref(info))
+    assert info.value == -2
+    n[1] = 8
+    J[20] = 0
+    assert not L.jk_batch_create(2, ip(n), ip(n2), ip(J), None, ctypes.byref(info))
+    assert info.value == -23
+    assert not L.jk_batch_create(0, ip(n), ip(n2), ip(J), None, ctypes.byref(info))
+    assert info.value == -1
