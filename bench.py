@@ -38,6 +38,9 @@ WORKLOADS = {
                      desc="Y iid N(0,1), seed 1; J = 192 x +1 then 64 x -1; N_2 = 128"),
     "zjk_n1024": dict(kind="complex", n=1024, n_2=512, make=lambda: gen.complex_gaussian(1024, seed=3),
                       desc="Y complex, Re/Im iid N(0,1/2), seed 3; J = 512 x +1 then 512 x -1; N_2 = 512"),
+    "batch4096": dict(kind="batch", count=4096, make=lambda seed=4: gen.batch(4096, 16, 128, seed=seed),
+                      desc="4096 real matrices, even N uniform in [16,128], Y iid N(0,1), J iid +-1 with "
+                           "P(+1) ~ U[0.2,0.8] per matrix, N_2 = N/2; seed 4 (+ rank); one persistent launch"),
 }
 STEPS_FILE = os.path.join(ROOT, "bench_steps.json")
 
@@ -113,10 +116,48 @@ def cpu_sample(Y, J, n_2, max_seconds=20.0):
     return dt / steps, steps, nt
 
 
+def cpu_batch_estimate(mats, steps, max_seconds=20.0):
+    """The oracle port on the host cores for a batch: per-step time measured at one thread
+    for a few orders (whole solver steps from the start of a solve), interpolated as
+    c N^3 + d, times each matrix's step count, divided by the cores (one matrix per core,
+    perfect scaling assumed).  Returns (seconds for the batch, cores, sample description)."""
+    import oracle
+    cores = os.cpu_count() or 1
+    ns = sorted({int(Y.shape[0]) for Y in mats})
+    probe = [ns[0], ns[len(ns) // 2], ns[-1]]
+    per = {}
+    budget = max_seconds / len(probe)
+    for n in probe:
+        Y, J = next((Y, J) for Y, J in zip(mats, _batch_js) if Y.shape[0] == n)
+        t0 = time.perf_counter()
+        k = 4
+        oracle.step_loop(Y, J, nt=1, stop_after=k)
+        dt = time.perf_counter() - t0
+        k = max(4, min(2000, int(budget / max(dt / 4, 1e-6))))
+        t0 = time.perf_counter()
+        oracle.step_loop(Y, J, nt=1, stop_after=k)
+        per[n] = (time.perf_counter() - t0) / k
+    x = np.array([float(n) ** 3 for n in probe])
+    y = np.array([per[n] for n in probe])
+    c, d = np.polyfit(x, y, 1)
+    d = max(d, 0.0)
+    cap = 4000 * max(int(Y.shape[0]) for Y in mats) + 100000  # the library's default step limit
+    tot = sum((int(st) if st > 0 else (cap if st == -24 else 1)) * (c * float(Y.shape[0]) ** 3 + d)
+              for Y, st in zip(mats, steps))
+    desc = (f"oracle steps timed at 1 thread for N in {probe} ({', '.join(f'{per[n] * 1e3:.3f}' for n in probe)} "
+            f"ms/step), fitted c N^3 + d, x each matrix's step count, / {cores} cores")
+    return tot / cores, cores, desc
+
+
+_batch_js = []
+
+
 def run_reference(args, wl):
     ws, rank, _ = _dist()
     if rank != 0:
         return
+    if wl["kind"] == "batch":
+        return run_reference_batch(args, wl)
     Y, J = wl["make"]()
     rec = _steps_record().get(args.workload)
     if not rec:
@@ -140,6 +181,145 @@ def run_reference(args, wl):
                                    f"multiplied by the {rec} steps the solve takes"},
         "e2e": {"value": 1.0 / solve_s, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    print(json.dumps(out))
+
+
+def run_reference_batch(args, wl):
+    rec = _steps_record().get(args.workload)
+    if not rec:
+        print(json.dumps({"impl": "reference", "unavailable": "no recorded step counts for this workload"}))
+        return
+    b = wl["make"]()
+    mats = [Y for Y, _ in b]
+    _batch_js[:] = [J for _, J in b]
+    per = []
+    for _ in range(args.warmup):
+        cpu_batch_estimate(mats, rec, max_seconds=3.0)
+    for _ in range(args.steps):
+        sec, cores, desc = cpu_batch_estimate(mats, rec, max_seconds=20.0)
+        per.append(sec)
+    sec = float(np.mean(per))
+    out = {
+        "impl": "reference", "metric": "HSVD time-to-converge & solves/s", "value": len(mats) / sec, "unit": "solves/s",
+        "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": {"workload": args.workload, "desc": wl["desc"]},
+        "cpu_baseline": {"value": len(mats) / sec, "unit": "solves/s", "cores": cores, "kind": "port", "sample": desc},
+        "e2e": {"value": len(mats) / sec, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out))
+
+
+def run_ours_batch(args, wl):
+    import torch
+    import torch.distributed as dist
+
+    import jkogb_b200 as jk
+
+    ws, rank, local = _dist()
+    if ws > 1:
+        torch.cuda.set_device(local)
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=900), device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    b = wl["make"](seed=4 + rank)  # one batch per rank: the ranks partition the job, no collective on the data path
+    mats = [Y for Y, _ in b]
+    Js = [J for _, J in b]
+    A, J, n, off = jk.batch_pack(mats, Js)
+    cnt = len(n)
+    plan = jk.Batch(n, np.zeros(cnt, np.int32), J)
+    A0 = torch.from_numpy(A).to(dev)
+    dA = A0.clone()
+    dU = torch.empty_like(dA)
+    dZ = torch.empty_like(dA)
+    ds = torch.empty(int(n.sum()), dtype=torch.float64, device=dev)
+    di = torch.zeros(cnt, dtype=torch.int32, device=dev)
+    side = torch.cuda.Stream(dev)
+    st = side.cuda_stream
+    ptrs = (dA.data_ptr(), dU.data_ptr(), dZ.data_ptr(), ds.data_ptr(), di.data_ptr())
+
+    def barrier():
+        if ws > 1:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+
+    threads = plan.tune(*ptrs, st)
+    for _ in range(args.warmup):
+        with torch.cuda.stream(side):
+            dA.copy_(A0)
+        plan.run(*ptrs, st)
+    barrier()
+    smi, smf = _clock_sampler(local)
+    ev = []
+    launches = 0
+    for k in range(args.steps):
+        with torch.cuda.stream(side):
+            dA.copy_(A0)  # restore the input, outside the timed launch
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(side)
+        plan.run(*ptrs, st)
+        e1.record(side)
+        ev.append((e0, e1))
+        launches += 1
+    barrier()
+    clocks = _clock_summary(smi, smf)
+    dev_ms = sum(a.elapsed_time(b) for a, b in ev)
+    t = torch.tensor([dev_ms], dtype=torch.float64, device=dev)
+    if ws > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms = float(t.item()) / args.steps
+    info = di.cpu().numpy()
+    plan.close()
+
+    # end to end: the host-pointer entry (copies in and out inside the call)
+    barrier()
+    tt0 = time.perf_counter()
+    for _ in range(args.steps):
+        res = jk.dstep_loop_batched(mats, Js)
+    e2e_s = (time.perf_counter() - tt0) / args.steps
+    te = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
+    if ws > 1:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_s = float(te.item())
+    same = bool(np.array_equal(np.array([r["info"] for r in res]), info))
+
+    # FP64 work of the weight scans of the whole batch: sum over matrices and steps of
+    # NH (N - 2) 14 flop, with each matrix's NH and step count
+    nplus = np.array([int(np.sum(j == 1)) for j in Js])
+    steps_pos = np.where(info > 0, info, 0).astype(np.float64)
+    flops = float(np.sum(steps_pos * nplus * (n - nplus) * (n - 2) * 14.0))
+    achieved = flops / (ms * 1e-3) / 1e12
+    peak = jk.lib().jk_fp64_peak()
+    if ws > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    out = {
+        "metric": "HSVD time-to-converge & solves/s", "value": ws * cnt * 1e3 / ms, "unit": "solves/s",
+        "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded generator, the workload's distributions)",
+        "config": {"workload": args.workload, "desc": wl["desc"], "matrices": cnt, "threads_per_block": threads,
+                   "parallelism": f"partition{ws}", "steps_total": int(steps_pos.sum()),
+                   "matrices_over_100N_steps": int(np.sum(info > 100 * n)), "matrices_step_capped": int(np.sum(info == -24)),
+                   "l2": "each block's matrix lives in shared memory; U, Z (<= 0.5 GB) stream through L2"},
+        "e2e": {"value": ws * cnt / e2e_s, "unit": "solves/s", "h2d_bytes_per_step": int(A.nbytes + J.nbytes),
+                "d2h_bytes_per_step": int(3 * A.nbytes + 8 * int(n.sum()) + 4 * cnt), "same_info": same},
+        "gpu_launches": launches,
+        "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                     "frac": achieved / peak if peak > 0 else None, "traffic": None,
+                     "kernel": "k_batch (the whole batched solve, one launch)",
+                     "algorithmic_flop_per_launch": flops, "launch_ms": ms,
+                     "peak_note": "counts only the weight scans (NH (N-2) 14 flop per step); FP64 FMA peak measured "
+                                  "live by jk_fp64_peak"},
+        "clocks": clocks,
+    }
+    if args.cpu_baseline:
+        _batch_js[:] = Js
+        sec, cores, desc = cpu_batch_estimate(mats, info, max_seconds=20.0)
+        out["cpu_baseline"] = {"value": cnt / sec, "unit": "solves/s", "cores": cores, "kind": "port", "sample": desc}
     print(json.dumps(out))
 
 
@@ -285,6 +465,8 @@ def main():
     wl = WORKLOADS[args.workload]
     if args.impl == "reference":
         run_reference(args, wl)
+    elif wl["kind"] == "batch":
+        run_ours_batch(args, wl)
     else:
         run_ours(args, wl)
 

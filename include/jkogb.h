@@ -138,9 +138,10 @@ void jk_batch_destroy(jk_batch *b);
  * SIGMA, INFO out.  The launch is captured once per set of buffers as a CUDA graph
  * and replayed.  Returns 0 or an error; does not synchronise. */
 int jk_batch_run(jk_batch *b, double *dA, double *dU, double *dZ, double *dsigma, int *dinfo, void *stream);
-/* Autotune the block shape (threads per block) on this batch: solves a copy of dA with
- * every candidate, keeps the fastest for later runs and returns its thread count.  dA
- * is left unchanged; dU, dZ, dsigma, dinfo receive a solve's outputs. */
+/* Autotune the block shape (threads per block) on this batch: times every candidate on
+ * a copy of the batch's largest matrices (two per resident block, at most 30 N steps
+ * each), keeps the fastest for later runs and returns its thread count.  dA is left
+ * unchanged; dU, dZ, dsigma, dinfo are overwritten (scratch). */
 int jk_batch_tune(jk_batch *b, const double *dA, double *dU, double *dZ, double *dsigma, int *dinfo, void *stream);
 /* The same with host buffers (copies in and out, synchronous).  Returns 0 or an error. */
 int jk_dstep_loop_batched(int count, const int *n, const int *n_2, double *A, double *U, double *Z, const int *J,

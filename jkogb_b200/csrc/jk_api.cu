@@ -562,13 +562,17 @@ int jk_batch_tune(jk_batch *b, const double *dA, double *dU, double *dZ, double 
   float best_ms = -1.0f;
   int best = b->variant;
   cudaError_t err = cudaSuccess;
+  // time a bounded sample: the first (largest) matrices of the work order, two per
+  // resident block, each stopped after at most 30 N steps
+  const long long cap_t = (b->cap < 30LL * b->nm) ? b->cap : 30LL * b->nm;
   for (int v = 0; v < kBatchVariants && err == cudaSuccess; ++v) {
     const int grid = batch_grid(v, b->nm);
     if (grid <= 0) continue;
+    const int sub = (b->count < 2 * grid) ? b->count : 2 * grid;
     err = cudaMemcpyAsync(scratch, dA, b->total * sizeof(double), cudaMemcpyDeviceToDevice, s);
     if (err == cudaSuccess) err = cudaEventRecord(e0, s);
     if (err == cudaSuccess)
-      err = launch_batch(v, grid, b->items, b->count, b->counter, scratch, dU, dZ, b->J, dsigma, dinfo, b->nm, b->cap, s);
+      err = launch_batch(v, grid, b->items, sub, b->counter, scratch, dU, dZ, b->J, dsigma, dinfo, b->nm, cap_t, s);
     if (err == cudaSuccess) err = cudaEventRecord(e1, s);
     if (err == cudaSuccess) err = cudaEventSynchronize(e1);
     float ms = 0.0f;

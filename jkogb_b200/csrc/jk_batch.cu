@@ -11,9 +11,10 @@
 //   weights    DMAGF2T / DMAGF2H (+ ABODNDF2) of every pair, the arithmetic of the
 //              single-matrix kernels (src/D/dstep.F90:12-72, 189-219)
 //   selection  the greedy non-colliding pivots (AW_SRT* + AW_NCP1/2,
-//              src/shared/atypes.F90:85-484) as the greedy matching, in rounds of
-//              mutual best proposals; a vertex rescans only when its proposal was
-//              matched away; matched pairs ranked by the record order, first N_2 kept
+//              src/shared/atypes.F90:85-484) as the greedy matching, by the Suitor
+//              method (warp-wide proposals that displace worse suitors, shared-memory
+//              compare-and-swap, no barrier per round); matched pairs ranked by the
+//              record order, the first N_2 kept
 //   pivots     the 2x2 HSVDs (src/D/dstep.F90:301-326), NL and the error minimum
 //   rotations  all row rotations (BA) of A and the column rotations of U and Z, then,
 //              if no pivot failed, the column rotations (AB) of A and the diagonal
@@ -57,7 +58,7 @@ struct BLayout {
     jv = align16(vlist + (size_t)nm * sizeof(int));
     best = align16(jv + (size_t)nm * sizeof(int));
     ms = align16(best + (size_t)nm * sizeof(int));
-    total = align16(ms + (size_t)nm * 2);
+    total = ms;
   }
 };
 
@@ -84,12 +85,10 @@ __device__ void solve_one(const BatchItem &it, double *__restrict__ gA, double *
   int *pos = (int *)(smem + L.pos);      // vertex -> shared-memory column
   int *vl = (int *)(smem + L.vlist);     // shared-memory column -> vertex (+ columns, then - columns)
   int *Jv = (int *)(smem + L.jv);
-  int *best = (int *)(smem + L.best);
-  unsigned char *ms = smem + L.ms;       // 0 free, 1 matched, 2 retired (no free partner left)
-  unsigned char *rescan = ms + nm;
-  __shared__ int s_np, s_cnt, s_got, s_nl, s_err;
+  int *suitor = (int *)(smem + L.best);  // per vertex: its current suitor (-1: none)
+  __shared__ int s_np, s_cnt, s_nl, s_err;
 
-  const int tid = threadIdx.x, n = it.n, lda = n + 1;
+  const int tid = threadIdx.x, n = it.n, lda = n + 1, v_ = tid;
   double *A = gA + it.off, *U = gU + it.off, *Z = gZ + it.off;
   const int *J = gJ + it.joff;
 
@@ -185,49 +184,75 @@ __device__ void solve_one(const BatchItem &it, double *__restrict__ gA, double *
       if (w < -JK_HUGE) w = nan_w();
       Ws[tri(p, q)] = w;
     }
-    for (int v = tid; v < n; v += THREADS) { ms[v] = 0; rescan[v] = 1; best[v] = -1; }
+    for (int v = tid; v < n; v += THREADS) suitor[v] = -1;
     if (tid == 0) { s_cnt = 0; s_nl = 0; s_err = 0; }
     __syncthreads();
 
-    // ---- selection: rounds of mutual best proposals (the greedy matching)
-    for (;;) {
-      for (int v = tid; v < n; v += THREADS) {
-        if (ms[v] || !rescan[v]) continue;
-        int bu = -1;
-        double bw = 0.0;
-        unsigned bt = 0;
-        for (int u = 0; u < n; ++u) {
-          if (u == v || ms[u]) continue;
-          const int p = (u < v) ? u : v, q = (u < v) ? v : u;
-          const double w = Ws[tri(p, q)];
-          if (w != w) continue;  // NaN: no record
-          const unsigned t = rtie(p, q);
-          if (bu < 0 || rbetter(w, t, bw, bt)) { bu = u; bw = w; bt = t; }
+    // ---- selection: the greedy matching by the Suitor method (Manne & Halappanavar):
+    // a vertex proposes to its best partner whose current suitor offers a worse pair
+    // (record order), displacing that suitor, which then proposes in turn.  With a
+    // strict total order this ends in the greedy matching, the set of pairs the walk
+    // over the sorted records takes, without a barrier per round.  A warp makes one
+    // proposal at a time: its lanes scan the partners, a butterfly reduction finds
+    // the best open one, lane 0 places it with a compare-and-swap.
+    {
+      volatile int *vs = suitor;  // other warps change it at any time
+      const int lane = tid & 31;
+      int guard = 0;
+      const int limit = 2 * n * n + 64;
+      for (int v0 = tid >> 5; v0 < n && guard <= limit; v0 += THREADS / 32) {
+        int cur = v0;
+        while (cur >= 0 && guard <= limit) {
+          double bw = 0.0;
+          unsigned bt = 0u;
+          int bu = -1;
+          for (int u = lane; u < n; u += 32) {
+            if (u == cur) continue;
+            const int p = (u < cur) ? u : cur, q = (u < cur) ? cur : u;
+            const double w = Ws[tri(p, q)];
+            if (w != w) continue;  // NaN: no record
+            const unsigned t = rtie(p, q);
+            if (bu >= 0 && !rbetter(w, t, bw, bt)) continue;
+            const int su = vs[u];
+            if (su >= 0) {
+              const int p2 = (u < su) ? u : su, q2 = (u < su) ? su : u;
+              if (!rbetter(w, t, Ws[tri(p2, q2)], rtie(p2, q2))) continue;
+            }
+            bw = w; bt = t; bu = u;
+          }
+#pragma unroll
+          for (int off = 16; off > 0; off >>= 1) {
+            const double ow = __shfl_xor_sync(0xFFFFFFFFu, bw, off);
+            const unsigned ot = __shfl_xor_sync(0xFFFFFFFFu, bt, off);
+            const int ou = __shfl_xor_sync(0xFFFFFFFFu, bu, off);
+            if (ou >= 0 && (bu < 0 || rbetter(ow, ot, bw, bt))) { bw = ow; bt = ot; bu = ou; }
+          }
+          if (bu < 0) break;  // no open partner: cur stays unmatched
+          int res = -2;
+          if (lane == 0) {
+            const int s0 = vs[bu];
+            bool still = (s0 < 0);
+            if (!still) {
+              const int p2 = (bu < s0) ? bu : s0, q2 = (bu < s0) ? s0 : bu;
+              still = rbetter(bw, bt, Ws[tri(p2, q2)], rtie(p2, q2));
+            }
+            if (still && atomicCAS(&suitor[bu], s0, cur) == s0) res = s0;
+          }
+          res = __shfl_sync(0xFFFFFFFFu, res, 0);
+          ++guard;
+          if (res == -2) continue;  // overtaken meanwhile: look again
+          cur = res;                // the displaced suitor proposes next
         }
-        best[v] = bu;
-        rescan[v] = 0;
       }
-      if (tid == 0) s_got = 0;
-      __syncthreads();
-      for (int v = tid; v < n; v += THREADS) {
-        if (ms[v]) continue;
-        const int u = best[v];
-        if (u < 0) { ms[v] = 2; continue; }
-        if (v < u && best[u] == v) {
-          ms[v] = 1;
-          ms[u] = 1;
-          pairs[atomicAdd(&s_cnt, 1)] = make_int2(v, u);
-          atomicAdd(&s_got, 1);
-        }
-      }
-      __syncthreads();
-      const int got = s_got;
-      if (!got) break;
-      // a proposal stays the best free partner while its target is free
-      for (int v = tid; v < n; v += THREADS)
-        if (!ms[v] && best[v] >= 0 && ms[best[v]]) rescan[v] = 1;
-      __syncthreads();
+      if (guard > limit && lane == 0) atomicMin(&s_err, kInfoSelect);
     }
+    __syncthreads();
+    if (v_ < n) {
+      const int u = suitor[v_];
+      if (u > v_ && suitor[u] == v_) pairs[atomicAdd(&s_cnt, 1)] = make_int2(v_, u);
+    }
+    __syncthreads();
+    if (s_err < 0) { info = s_err; break; }
     // rank the matched pairs by the record order; the first N_2 are the pivots
     const int cnt = s_cnt, sl = (cnt < it.n_2) ? cnt : it.n_2;
     for (int r = tid; r < cnt; r += THREADS) {

@@ -99,6 +99,7 @@ struct BatchItem {
 constexpr int kBatchMaxN = 128;
 constexpr int kBatchVariants = 3;
 constexpr int kInfoMaxSteps = -24;
+constexpr int kInfoSelect = -25;  // the batched selection exceeded its iteration bound (internal error)
 extern const int kBatchThreads[kBatchVariants];
 size_t batch_smem(int nm);
 cudaError_t batch_prepare(int nm);
