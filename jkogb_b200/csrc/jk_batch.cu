@@ -71,6 +71,33 @@ __device__ __forceinline__ bool rbetter(double w1, unsigned t1, double w2, unsig
 
 __device__ __forceinline__ unsigned rtie(int p, int q) { return ((unsigned)(q - p) << 16) | (unsigned)p; }
 
+// ABODNDF2's sequential sum over the rows i != p, q of the columns xs (p), ys (q)
+// under the AB coefficients t (src/D/dtransf.F90:246-348)
+__device__ __forceinline__ void scan_pair(const double *xs, const double *ys, int n, int p, int q, const Rot &t, double &d)
+{
+  if (t.c1 && t.c2) {
+#pragma unroll 4
+    for (int i = 0; i < n; ++i) {
+      const double x = xs[i], y = ys[i];
+      const double xx = __dmul_rn(fma(y, t.r1, x), t.m1);
+      const double yy = __dmul_rn(fma(x, t.r2, y), t.m2);
+      const double e1 = fma(__dsub_rn(x, xx), __dadd_rn(x, xx), d);
+      const double e2 = fma(__dsub_rn(y, yy), __dadd_rn(y, yy), e1);
+      d = (i != p && i != q) ? e2 : d;
+    }
+  }
+  else {
+    for (int i = 0; i < n; ++i) {
+      double x = xs[i], y = ys[i];
+      const double x0 = x, y0 = y;
+      rot_apply(t, x, y);
+      const double e1 = fma(__dsub_rn(x0, x), __dadd_rn(x0, x), d);
+      const double e2 = fma(__dsub_rn(y0, y), __dadd_rn(y0, y), e1);
+      d = (i != p && i != q) ? e2 : d;
+    }
+  }
+}
+
 template <int THREADS>
 __device__ void solve_one(const BatchItem &it, double *__restrict__ gA, double *__restrict__ gU, double *__restrict__ gZ,
                           const int *__restrict__ gJ, double *__restrict__ gsigma, int *__restrict__ ginfo, int nm,
@@ -146,43 +173,76 @@ __device__ void solve_one(const BatchItem &it, double *__restrict__ gA, double *
       else w = (nz || (app < aqq)) ? dasum2(aqp, apq) : nan_w();
       Ws[k] = w;
     }
-    // ---- weights of the hyperbolic pairs (DMAGF2H + ABODNDF2): + column ci, - column cj
+    // ---- weights of the hyperbolic pairs (DMAGF2H + ABODNDF2): + column ci, - column cj;
+    // with up to 384 threads two pairs per thread, their fma chains interleaved (the
+    // 512-thread shape has no registers to spare for it)
     const int nh = np * nmn;
-    for (int k = tid; k < nh; k += THREADS) {
-      const int ci = k / nmn, cj = np + k % nmn;  // shared-memory columns
-      const int a = vl[ci], b = vl[cj];
-      const bool a_is_p = a < b;
-      const int p = a_is_p ? a : b, q = a_is_p ? b : a;
-      const double *xs = As + (a_is_p ? ci : cj) * lda, *ys = As + (a_is_p ? cj : ci) * lda;
-      double w, d = 0.0;
-      Rot t;
-      if (hyp_setup(xs[p], xs[q], ys[p], ys[q], a_is_p ? 1 : -1, w, d, t)) {
-        // ABODNDF2's sequential sum over the rows i != p, q
-        if (t.c1 && t.c2) {
-#pragma unroll 4
-          for (int i = 0; i < n; ++i) {
-            const double x = xs[i], y = ys[i];
-            const double xx = __dmul_rn(fma(y, t.r1, x), t.m1);
-            const double yy = __dmul_rn(fma(x, t.r2, y), t.m2);
-            const double e1 = fma(__dsub_rn(x, xx), __dadd_rn(x, xx), d);
-            const double e2 = fma(__dsub_rn(y, yy), __dadd_rn(y, yy), e1);
-            d = (i != p && i != q) ? e2 : d;
-          }
+    if constexpr (THREADS > 384) {
+      for (int k = tid; k < nh; k += THREADS) {
+        const int ci = k / nmn, cj = np + k % nmn;  // shared-memory columns
+        const int a = vl[ci], b = vl[cj];
+        const bool a_is_p = a < b;
+        const int p = a_is_p ? a : b, q = a_is_p ? b : a;
+        const double *xs = As + (a_is_p ? ci : cj) * lda, *ys = As + (a_is_p ? cj : ci) * lda;
+        double w, d = 0.0;
+        Rot t;
+        if (hyp_setup(xs[p], xs[q], ys[p], ys[q], a_is_p ? 1 : -1, w, d, t)) {
+          scan_pair(xs, ys, n, p, q, t, d);
+          w = d;
         }
-        else {
-          for (int i = 0; i < n; ++i) {
-            double x = xs[i], y = ys[i];
-            const double x0 = x, y0 = y;
-            rot_apply(t, x, y);
-            const double e1 = fma(__dsub_rn(x0, x), __dadd_rn(x0, x), d);
-            const double e2 = fma(__dsub_rn(y0, y), __dadd_rn(y0, y), e1);
-            d = (i != p && i != q) ? e2 : d;
-          }
-        }
-        w = d;
+        if (w < -JK_HUGE) w = nan_w();
+        Ws[tri(p, q)] = w;
       }
-      if (w < -JK_HUGE) w = nan_w();
-      Ws[tri(p, q)] = w;
+    }
+    else
+    for (int k0 = tid; k0 < nh; k0 += 2 * THREADS) {
+      int pp[2], qq[2];
+      const double *xs[2], *ys[2];
+      double w[2], d[2];
+      Rot t[2];
+      bool sc[2];
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int k = k0 + h * THREADS;
+        sc[h] = false; w[h] = nan_w(); d[h] = 0.0; pp[h] = 0; qq[h] = 1; xs[h] = As; ys[h] = As;
+        if (k < nh) {
+          const int ci = k / nmn, cj = np + k % nmn;  // shared-memory columns
+          const int a = vl[ci], b = vl[cj];
+          const bool a_is_p = a < b;
+          pp[h] = a_is_p ? a : b;
+          qq[h] = a_is_p ? b : a;
+          xs[h] = As + (a_is_p ? ci : cj) * lda;
+          ys[h] = As + (a_is_p ? cj : ci) * lda;
+          sc[h] = hyp_setup(xs[h][pp[h]], xs[h][qq[h]], ys[h][pp[h]], ys[h][qq[h]], a_is_p ? 1 : -1, w[h], d[h], t[h]);
+        }
+      }
+      if (sc[0] && sc[1] && t[0].c1 && t[0].c2 && t[1].c1 && t[1].c2) {
+        // ABODNDF2's sequential sums over the rows i != p, q, two chains at once
+#pragma unroll 2
+        for (int i = 0; i < n; ++i) {
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const double x = xs[h][i], y = ys[h][i];
+            const double xx = __dmul_rn(fma(y, t[h].r1, x), t[h].m1);
+            const double yy = __dmul_rn(fma(x, t[h].r2, y), t[h].m2);
+            const double e1 = fma(__dsub_rn(x, xx), __dadd_rn(x, xx), d[h]);
+            const double e2 = fma(__dsub_rn(y, yy), __dadd_rn(y, yy), e1);
+            d[h] = (i != pp[h] && i != qq[h]) ? e2 : d[h];
+          }
+        }
+      }
+      else {
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+          if (sc[h]) scan_pair(xs[h], ys[h], n, pp[h], qq[h], t[h], d[h]);
+      }
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        if (k0 + h * THREADS >= nh) continue;
+        double x = sc[h] ? d[h] : w[h];
+        if (x < -JK_HUGE) x = nan_w();
+        Ws[tri(pp[h], qq[h])] = x;
+      }
     }
     for (int v = tid; v < n; v += THREADS) suitor[v] = -1;
     if (tid == 0) { s_cnt = 0; s_nl = 0; s_err = 0; }
