@@ -32,7 +32,9 @@ LIB_PATH = os.path.join(_HERE, "_lib", "libjkogb_b200.so")
 SYMBOLS = ("jk_dstep_loop", "jk_zstep_loop", "jk_dstep_loop_dev", "jk_zstep_loop_dev", "jk_dhsvd2_batch",
            "jk_zhsvd2_batch", "jk_dweights", "jk_zweights", "jk_select", "jk_handle_create", "jk_handle_destroy",
            "jk_handle_weights", "jk_dweights_noalloc", "jk_batch_create", "jk_batch_destroy",
-           "jk_batch_run", "jk_batch_tune", "jk_dstep_loop_batched", "jk_last_launch_count", "jk_fp64_peak", "jk_max_order", "jk_strerror")
+           "jk_batch_run", "jk_batch_tune", "jk_dstep_loop_batched", "jk_mlp_nparams", "jk_scorer_create",
+           "jk_scorer_destroy", "jk_dstep_loop_dev_scored", "jk_mlp_features", "jk_mlp_forward", "jk_mlp_grad_workspace",
+           "jk_mlp_grad", "jk_mlp_adam", "jk_last_launch_count", "jk_fp64_peak", "jk_max_order", "jk_strerror")
 
 
 class JkError(RuntimeError):
@@ -101,6 +103,25 @@ def lib():
         L.jk_batch_run.argtypes = [C.c_void_p, vp, vp, vp, vp, vp, vp]
         L.jk_batch_tune.restype = C.c_int
         L.jk_batch_tune.argtypes = [C.c_void_p, vp, vp, vp, vp, vp, vp]
+        L.jk_mlp_nparams.restype = C.c_int
+        L.jk_mlp_nparams.argtypes = [C.c_int]
+        L.jk_scorer_create.restype = C.c_void_p
+        L.jk_scorer_create.argtypes = [C.c_int, C.POINTER(C.c_float), C.c_int, ip]
+        L.jk_scorer_destroy.restype = None
+        L.jk_scorer_destroy.argtypes = [C.c_void_p]
+        L.jk_dstep_loop_dev_scored.restype = C.c_int
+        L.jk_dstep_loop_dev_scored.argtypes = [C.c_int, vp, vp, vp, ip, vp, C.c_int, C.c_void_p, C.POINTER(Opts),
+                                               C.POINTER(Trace), ip, vp]
+        L.jk_mlp_features.restype = C.c_longlong
+        L.jk_mlp_features.argtypes = [C.c_int, vp, ip, C.c_int, vp, vp]
+        L.jk_mlp_forward.restype = C.c_int
+        L.jk_mlp_forward.argtypes = [C.c_int, C.c_int, vp, vp, vp, vp]
+        L.jk_mlp_grad_workspace.restype = C.c_longlong
+        L.jk_mlp_grad_workspace.argtypes = [C.c_int, C.c_int]
+        L.jk_mlp_grad.restype = C.c_int
+        L.jk_mlp_grad.argtypes = [C.c_int, C.c_int, vp, vp, vp, vp, vp, vp, vp]
+        L.jk_mlp_adam.restype = C.c_int
+        L.jk_mlp_adam.argtypes = [C.c_int, vp, vp, vp, vp, C.c_int, C.c_float, C.c_float, C.c_float, C.c_float, vp]
         L.jk_dstep_loop_batched.restype = C.c_int
         L.jk_dstep_loop_batched.argtypes = [C.c_int, ip, ip, vp, vp, vp, ip, vp, ip, C.POINTER(Opts)]
         L.jk_last_launch_count.restype = C.c_longlong

@@ -135,9 +135,22 @@ int make_workspace(Guard &g, Workspace &w, int n, int cplx, const int *J, int tr
   return 0;
 }
 
+}  // namespace
+
+// the learned ranking's network on the device
+struct jk_scorer {
+  Guard g;
+  unsigned short *w = nullptr;  // BF16 weights
+  float *b = nullptr;           // FP32 biases
+  int nf = 0;
+  int stall_k = 8;
+};
+
+namespace {
+
 // the loop of DSTEP_LOOP / ZSTEP_LOOP on device buffers
 int run_loop(int cplx, int n, void *dU, void *dA, void *dZ, const int *J, double *dsigma, int n_2, int id_ncp, int id_tru,
-             const jk_opts *opts, jk_trace *trace, cudaStream_t s)
+             const jk_opts *opts, jk_trace *trace, cudaStream_t s, const jk_scorer *sc = nullptr, int *exact_steps = nullptr)
 {
   (void)id_ncp;
   (void)id_tru;
@@ -151,6 +164,21 @@ int run_loop(int cplx, int n, void *dU, void *dA, void *dZ, const int *J, double
   int rc = make_workspace(g, w, n, cplx, J, trace_on, trace ? trace->max_steps : 0, trace ? trace->max_piv : 0);
   if (rc) return rc;
   w.zba_quirk = (o.zba_quirk == 0) ? 1 : 0;
+  if (sc) {
+    // a learned solve: the scorer's device parameters, the off-norm buffers, the mode flags
+    w.learned = 1;
+    w.sc.w = sc->w;
+    w.sc.b = sc->b;
+    w.sc.nf = sc->nf;
+    CK(g.alloc(&w.offpart, kOffBlocks * sizeof(double)));
+    CK(g.alloc(&w.offcount, sizeof(int)));
+    CK(cudaMemset(w.offcount, 0, sizeof(int)));
+    State s1;
+    CK(cudaMemcpy(&s1, w.st, sizeof(State), cudaMemcpyDeviceToHost));
+    s1.learned = 1;
+    s1.stall_k = sc->stall_k;
+    CK(cudaMemcpy(w.st, &s1, sizeof(State), cudaMemcpyHostToDevice));
+  }
 
   g_launches = 2;  // state init, U = Z = I
   CK(launch_init(w, dU, dZ, s));
@@ -190,11 +218,13 @@ int run_loop(int cplx, int n, void *dU, void *dA, void *dZ, const int *J, double
       return cuda_fail(e);
     }
     launched += per_sync;
-    g_launches += (long long)per_sync * (kStepLaunches - ((w.n_plus > 0 && w.n_minus > 0) ? 0 : 1));
+    g_launches += (long long)per_sync * (kStepLaunches - ((w.n_plus > 0 && w.n_minus > 0) ? 0 : 1) +
+                                         (w.learned ? ((w.n_plus > 0 && w.n_minus > 0) ? 2 : 1) : 0));
     if (w.st_host->stop) { info = w.st_host->info; break; }
     if (w.st_host->steps >= cap || launched > 2 * cap + per_sync) { info = JK_ERR_MAX_STEPS; break; }
   }
   if (exec) cudaGraphExecDestroy(exec);
+  if (exact_steps) *exact_steps = w.st_host->exact_steps;
   g_launches += 2;  // sigma, J Z^T J
   CK(launch_finish(w, dA, dZ, dsigma, s));
   if (trace) {
@@ -621,6 +651,104 @@ int jk_dstep_loop_batched(int count, const int *n, const int *n_2, double *A, do
   if (s) cudaStreamDestroy(s);
   jk_batch_destroy(b);
   return rc;
+}
+
+// ---------------------------------------------------------------------------
+// the learned ranking: scorer objects, the scored loop, training kernels
+// ---------------------------------------------------------------------------
+int jk_mlp_nparams(int nf) { return (nf == kMlpFeat) ? mlp_params(nf) : -1; }
+
+jk_scorer *jk_scorer_create(int nf, const float *params, int stall_k, int *info)
+{
+  int rc = 0;
+  if (nf != kMlpFeat) rc = -1;
+  else if (!params) rc = -2;
+  else if (stall_k < 1) rc = -3;
+  if (!rc) rc = pick_device(nullptr);
+  jk_scorer *sc = nullptr;
+  if (!rc) {
+    sc = new jk_scorer;
+    sc->nf = nf;
+    sc->stall_k = stall_k;
+    const int np = mlp_params(nf);
+    float *tmp = nullptr;
+    Guard g;
+    cudaError_t e = g.alloc(&tmp, np * sizeof(float));
+    if (e == cudaSuccess) e = sc->g.alloc(&sc->w, (kMlpHidden * nf + kMlpHidden * kMlpHidden + kMlpHidden) * sizeof(unsigned short));
+    if (e == cudaSuccess) e = sc->g.alloc(&sc->b, (2 * kMlpHidden + 1) * sizeof(float));
+    if (e == cudaSuccess) e = cudaMemcpy(tmp, params, np * sizeof(float), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = mlp_pack(nf, tmp, sc->w, sc->b, 0);
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) { rc = cuda_fail(e); delete sc; sc = nullptr; }
+  }
+  if (info) *info = rc;
+  return sc;
+}
+
+void jk_scorer_destroy(jk_scorer *sc) { delete sc; }
+
+int jk_dstep_loop_dev_scored(int n, double *dU, double *dA, double *dZ, const int *J, double *dsigma, int n_2,
+                             const jk_scorer *sc, const jk_opts *opts, jk_trace *trace, int *exact_steps, void *stream)
+{
+  if (!sc) return -9;
+  const int rc = check_args(n, n, n, n, J, n_2, 0, 0, 0);
+  if (rc) return rc;
+  return run_loop(0, n, dU, dA, dZ, J, dsigma, n_2, 0, 0, opts, trace, (cudaStream_t)stream, sc, exact_steps);
+}
+
+long long jk_mlp_features(int n, const double *dA, const int *J, int step, float *dX, void *stream)
+{
+  if (n < 3 || !dA || !J || !dX) return -1;
+  std::vector<int> plus, minus;
+  for (int i = 0; i < n; ++i) {
+    if (J[i] == 1) plus.push_back(i);
+    else if (J[i] == -1) minus.push_back(i);
+    else return JK_ERR_J;
+  }
+  const long long cnt = (long long)plus.size() * (long long)minus.size();
+  if (!cnt) return 0;
+  Guard g;
+  int *dp = nullptr, *dm = nullptr;
+  cudaStream_t s = (cudaStream_t)stream;
+  CK(g.alloc(&dp, plus.size() * sizeof(int)));
+  CK(g.alloc(&dm, minus.size() * sizeof(int)));
+  CK(cudaMemcpy(dp, plus.data(), plus.size() * sizeof(int), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(dm, minus.data(), minus.size() * sizeof(int), cudaMemcpyHostToDevice));
+  CK(mlp_features(n, dA, dp, dm, (int)plus.size(), (int)minus.size(), step, kMlpFeat, dX, s));
+  CK(cudaStreamSynchronize(s));  // the index lists are freed on return
+  return cnt;
+}
+
+int jk_mlp_forward(int nf, int count, const float *dX, const float *dParams, float *dY, void *stream)
+{
+  if (nf != kMlpFeat) return -1;
+  if (count < 0) return -2;
+  CK(mlp_forward(nf, count, dX, dParams, dY, (cudaStream_t)stream));
+  return 0;
+}
+
+long long jk_mlp_grad_workspace(int nf, int count)
+{
+  if (nf != kMlpFeat || count <= 0) return -1;
+  return (long long)mlp_grad_partial_floats(nf, count);
+}
+
+int jk_mlp_grad(int nf, int count, const float *dX, const float *dT, const float *dParams, float *dGrad, float *dLoss,
+                float *dWork, void *stream)
+{
+  if (nf != kMlpFeat) return -1;
+  if (count <= 0) return -2;
+  if (!dX || !dT || !dParams || !dGrad || !dLoss || !dWork) return -3;
+  CK(mlp_grad(nf, count, dX, dT, dParams, dGrad, dLoss, dWork, (cudaStream_t)stream));
+  return 0;
+}
+
+int jk_mlp_adam(int np, float *dParams, const float *dGrad, float *dM, float *dV, int t, float lr, float beta1,
+                float beta2, float eps, void *stream)
+{
+  if (np <= 0 || t < 1) return -1;
+  CK(mlp_adam(np, dParams, dGrad, dM, dV, t, lr, beta1, beta2, eps, (cudaStream_t)stream));
+  return 0;
 }
 
 long long jk_last_launch_count(void) { return g_launches; }

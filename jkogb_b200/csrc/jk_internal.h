@@ -26,6 +26,14 @@ struct State {
   long long trace_cap_piv;
   double tw;   // sum of the weights of the effective pivots (NORMF2D column)
   int trig, hyp;
+  // the learned ranking (jk_scorer): off unless `learned`
+  int learned;       // the solve ranks the scanned hyperbolic pairs by the scorer
+  int learned_step;  // this step uses the scorer (0: the exact weights)
+  int stall;         // steps since the off-norm last reached a new minimum
+  int stall_k;       // after this many such steps the next step is exact
+  int exact_steps;   // steps run with the exact weights in a learned solve
+  int retry;         // a learned step without an effective pivot: the loop goes on with an exact step
+  double off, best_off;  // off-norm after the last step, its minimum so far
 };
 
 // Per-step trace on the device (optional).
@@ -60,6 +68,13 @@ struct HypPar {
   int pad;
 };
 
+// the scorer of a learned solve (device parameters)
+struct ScorerDev {
+  const unsigned short *w;  // bf16 weights W1 [64][nf], W2 [64][64], W3 [64]
+  const float *b;           // fp32 biases b1 [64], b2 [64], b3
+  int nf;
+};
+
 struct Workspace {
   int n;
   int cplx;
@@ -79,6 +94,10 @@ struct Workspace {
   State *st_host;    // pinned host mirror
   Trace tr;
   int zba_quirk;
+  double *offpart;   // per-block partial off-norms (learned solves)
+  int *offcount;     // blocks done (the last one finishes the off-norm)
+  int learned;       // rank the scanned hyperbolic pairs by `sc`
+  ScorerDev sc;
 };
 
 // host launchers (jk_kernels.cu)
@@ -106,6 +125,23 @@ cudaError_t batch_prepare(int nm);
 int batch_blocks_per_sm(int variant, int nm);
 cudaError_t launch_batch(int variant, int grid, const BatchItem *items, int count, int *counter, double *A, double *U,
                          double *Z, const int *J, double *sigma, int *info, int nm, long long cap, cudaStream_t s);
+
+// the learned ranking (jk_scorer.cu)
+constexpr int kMlpHidden = 64;
+constexpr int kMlpFeat = 7;
+__host__ __device__ constexpr int mlp_params(int nf) { return kMlpHidden * nf + kMlpHidden + kMlpHidden * kMlpHidden + kMlpHidden + kMlpHidden + 1; }
+cudaError_t launch_learned_weights(Workspace &w, const double *A, cudaStream_t s);
+constexpr int kOffBlocks = 296;  // fixed grid of the off-norm reduction (a fixed summation order)
+cudaError_t launch_offnorm(Workspace &w, const double *A, cudaStream_t s);
+cudaError_t mlp_features(int n, const double *A, const int *plus, const int *minus, int n_plus, int n_minus, int step, int nf,
+                         float *X, cudaStream_t s);
+cudaError_t mlp_forward(int nf, int count, const float *X, const float *params, float *Y, cudaStream_t s);
+cudaError_t mlp_grad(int nf, int count, const float *X, const float *T, const float *params, float *grad, float *loss,
+                     float *partial, cudaStream_t s);
+size_t mlp_grad_partial_floats(int nf, int count);
+cudaError_t mlp_adam(int np, float *params, const float *grad, float *m, float *v, int t, float lr, float b1, float b2,
+                     float eps, cudaStream_t s);
+cudaError_t mlp_pack(int nf, const float *params, unsigned short *w, float *b, cudaStream_t s);
 
 // weights of a real matrix with no allocation: scratch in a static device array
 constexpr int kNoallocMaxN = 1024;

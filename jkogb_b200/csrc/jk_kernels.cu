@@ -49,11 +49,16 @@ __global__ void k_state_init(State *st)
 {
   const int cap_s = st->trace_cap_steps, on = st->trace_on;
   const long long cap_p = st->trace_cap_piv;
+  const int learned = st->learned, stall_k = st->stall_k;
   State z = {};
   z.trace_on = on;
   z.trace_cap_steps = cap_s;
   z.trace_cap_piv = cap_p;
   z.tw = -0.0;
+  z.learned = learned;
+  z.learned_step = learned;
+  z.stall_k = stall_k;
+  z.best_off = __longlong_as_double(0x7FF0000000000000LL);  // +inf
   *st = z;
 }
 
@@ -284,7 +289,7 @@ __global__ void __launch_bounds__(SCAN_THREADS, 2)
 k_hyp_tile(const State *st, const double *__restrict__ A, const int *__restrict__ J, int n, double *__restrict__ Wm,
            HypPar *par)
 {
-  if (st->stop) return;
+  if (st->stop || st->learned_step) return;  // a learned step ranks these pairs by the scorer
   const int T = (n + TW - 1) / TW;
   int tp, tq;
   tile_of(blockIdx.x, T, tp, tq);
@@ -431,7 +436,7 @@ __global__ void __launch_bounds__(HP * HM)
 k_weights_hyp(const State *st, const T *__restrict__ A, const int *__restrict__ plus, const int *__restrict__ minus,
               int n_plus, int n_minus, double *__restrict__ Wm, int n)
 {
-  if (st->stop) return;
+  if (st->stop || st->learned_step) return;  // a learned step ranks these pairs by the scorer
   __shared__ T sP[HP][HR + 1];
   __shared__ T sM[HM][HR + 1];
   const int tx = threadIdx.x % HP, ty = threadIdx.x / HP;
@@ -726,7 +731,12 @@ __device__ void end_of_step(State *st, const Piv<T> *piv, const int *J, Trace &t
       if (st->trace_npiv < st->trace_cap_piv) tr.piv[st->trace_npiv++] = make_int2(piv[i].p, piv[i].q);
   }
   if (err < 0) { st->info = err; st->stop = 1; }
-  else if (((sl < nl) ? sl : nl) <= 0) { st->info = st->steps; st->stop = 1; }
+  else if (((sl < nl) ? sl : nl) <= 0) {
+    // only a step ranked by the exact weights ends the loop; a learned step without an
+    // effective pivot is followed by an exact one
+    if (st->retry) st->retry = 0;
+    else { st->info = st->steps; st->stop = 1; }
+  }
   else st->steps += 1;
 }
 
@@ -1154,10 +1164,19 @@ static cudaError_t step_t(Workspace &w, T *A, T *U, T *Z, int n_2, cudaStream_t 
   const int n = w.n;
   cudaError_t e = weights_t(w, (const T *)A, s);
   if (e != cudaSuccess) return e;
+  if constexpr (sizeof(T) == sizeof(double)) {
+    // a learned solve: the scorer ranks the scanned hyperbolic pairs (the exact scan
+    // kernels above return at once in its learned steps)
+    if (w.learned && (e = launch_learned_weights(w, (const double *)A, s)) != cudaSuccess) return e;
+  }
   e = select_t(w, (const T *)A, n_2, s);
   if (e != cudaSuccess) return e;
   k_rotate<T><<<(n + 1) / 2, 256, 2 * (size_t)n * sizeof(T), s>>>(w.st, A, U, Z, n, (const Piv<T> *)w.piv,
                                                                  (const RowRot<T> *)w.rowrot, w.unp);
+  if constexpr (sizeof(T) == sizeof(double)) {
+    if (w.learned && (e = cudaGetLastError()) == cudaSuccess) e = launch_offnorm(w, (const double *)A, s);
+    if (e != cudaSuccess) return e;
+  }
   return cudaGetLastError();
 }
 

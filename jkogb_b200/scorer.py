@@ -1,0 +1,203 @@
+"""The learned ranking: training data from the exact method's trajectories, training
+with the library's own forward/backward/Adam kernels, and the scored solve.
+
+The network (7 -> 64 -> 64 -> 1, ReLU, BF16 weights, FP32 biases and accumulation)
+predicts g(w) = sign(w) (log2|w| + 1100) / 1024 of a hyperbolic pair's exact weight w
+(DMAGF2H, src/D/dstep.F90:41-72) from the pair's 2x2 block; g is monotone, so ranking
+by the prediction ranks by the predicted weight.  Device memory here is torch's; all
+arithmetic runs in the library's kernels (jk_mlp_*).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import JkError, Handle, Opts, _opts, lib
+
+NF = 7
+HIDDEN = 64
+
+
+def nparams() -> int:
+    return int(lib().jk_mlp_nparams(NF))
+
+
+def g_of(w):
+    """The training target of a weight: sign(w) (log2|w| + 1100) / 1024, 0 for w = 0."""
+    w = np.asarray(w, np.float64)
+    a = np.abs(w)
+    with np.errstate(divide="ignore"):
+        lg = np.where(a > 0, np.log2(np.where(a > 0, a, 1.0)), 0.0)
+    return np.where(a > 0, np.sign(w) * (lg + 1100.0) / 1024.0, 0.0)
+
+
+def init_params(seed=0) -> np.ndarray:
+    """He-initialised FP32 parameters in the library's layout (W1, b1, W2, b2, W3, b3)."""
+    r = np.random.Generator(np.random.PCG64(seed))
+    w1 = r.standard_normal((HIDDEN, NF)) * np.sqrt(2.0 / NF)
+    w2 = r.standard_normal((HIDDEN, HIDDEN)) * np.sqrt(2.0 / HIDDEN)
+    w3 = r.standard_normal(HIDDEN) * np.sqrt(1.0 / HIDDEN)
+    p = np.concatenate([w1.ravel(), np.zeros(HIDDEN), w2.ravel(), np.zeros(HIDDEN), w3, [0.0]]).astype(np.float32)
+    assert p.size == nparams()
+    return p
+
+
+def _vp(t):
+    return C.c_void_p(t.data_ptr())
+
+
+def _stream(torch, dev):
+    return C.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
+
+
+def features(dA, J, step):
+    """Features of every hyperbolic pair of the column-major device matrix dA (torch),
+    (+ index, - index) order; returns (X (count, 7) float32 on the device, plus, minus)."""
+    import torch
+    n = dA.shape[0]
+    Jc = np.ascontiguousarray(np.asarray(J, np.int32))
+    plus = np.nonzero(Jc == 1)[0]
+    minus = np.nonzero(Jc == -1)[0]
+    X = torch.empty((max(len(plus) * len(minus), 1), NF), dtype=torch.float32, device=dA.device)
+    cnt = lib().jk_mlp_features(n, _vp(dA), Jc.ctypes.data_as(C.POINTER(C.c_int)), int(step), _vp(X),
+                                _stream(torch, dA.device))
+    if cnt < 0:
+        raise JkError(int(cnt), "features: ")
+    return X[:cnt], plus, minus
+
+
+def forward(X, params):
+    """The network on device features X (count, 7); params a device float32 tensor."""
+    import torch
+    Y = torch.empty(X.shape[0], dtype=torch.float32, device=X.device)
+    rc = lib().jk_mlp_forward(NF, X.shape[0], _vp(X.contiguous()), _vp(params), _vp(Y), _stream(torch, X.device))
+    if rc < 0:
+        raise JkError(rc, "mlp forward: ")
+    return Y
+
+
+def grad(X, T, params):
+    """(loss, gradient) of the mean squared error, by the library's backward kernels."""
+    import torch
+    cnt = X.shape[0]
+    ws = int(lib().jk_mlp_grad_workspace(NF, cnt))
+    work = torch.empty(ws, dtype=torch.float32, device=X.device)
+    G = torch.empty_like(params)
+    loss = torch.empty(1, dtype=torch.float32, device=X.device)
+    rc = lib().jk_mlp_grad(NF, cnt, _vp(X.contiguous()), _vp(T.contiguous()), _vp(params), _vp(G), _vp(loss), _vp(work),
+                           _stream(torch, X.device))
+    if rc < 0:
+        raise JkError(rc, "mlp grad: ")
+    return loss, G
+
+
+def training_data(mats, Js, every=4, max_pairs=4096, seed=0):
+    """Features and targets along the exact method's trajectories: every `every`-th
+    step of each solve, up to max_pairs finite hyperbolic pairs per sampled step.
+    Returns (X, T) as device tensors."""
+    import torch
+    import jkogb_b200 as jk
+    r = np.random.Generator(np.random.PCG64(seed))
+    dev = torch.device("cuda", 0)
+    xs, ts = [], []
+    for Y, J in zip(mats, Js):
+        n = Y.shape[0]
+        A = torch.from_numpy(np.ascontiguousarray(np.asarray(Y).T)).to(dev).t().contiguous().t()
+        U = torch.empty_like(A)
+        Z = torch.empty_like(A)
+        s = torch.empty(n, dtype=torch.float64, device=dev)
+        W = torch.empty((n, n), dtype=torch.float64, device=dev).t()
+        h = Handle(n, J)
+        step = 0
+        while True:
+            X, plus, minus = features(A, J, step)
+            h.weights(A.data_ptr(), W.data_ptr(), torch.cuda.current_stream(dev).cuda_stream)
+            w = W[torch.from_numpy(plus).to(dev)][:, torch.from_numpy(minus).to(dev)].reshape(-1)
+            ok = torch.isfinite(w)
+            idx = torch.nonzero(ok).reshape(-1)
+            if idx.numel() == 0:
+                break
+            if idx.numel() > max_pairs:
+                idx = idx[torch.from_numpy(r.choice(idx.numel(), max_pairs, replace=False)).to(dev)]
+            xs.append(X[idx].clone())
+            ts.append(torch.from_numpy(g_of(w[idx].cpu().numpy()).astype(np.float32)).to(dev))
+            info = jk.step_loop_dev(A, U, Z, s, J, max_steps=every)
+            if info != -24:
+                break
+            A.diagonal().copy_(s)  # the loop leaves the diagonal in SIGMA
+            step += every
+        h.close()
+    return torch.cat(xs), torch.cat(ts)
+
+
+def train(X, T, params=None, iters=2000, batch=8192, lr=2e-3, seed=0, log=None):
+    """Adam on the mean squared error with the library's kernels; returns the FP32
+    parameters (numpy) and the loss history."""
+    import torch
+    dev = X.device
+    P = torch.from_numpy(init_params(seed) if params is None else np.asarray(params, np.float32)).to(dev)
+    M = torch.zeros_like(P)
+    V = torch.zeros_like(P)
+    g = torch.Generator(device="cpu").manual_seed(seed)
+    hist = []
+    cnt = X.shape[0]
+    L = lib()
+    st = _stream(torch, dev)
+    for it in range(1, iters + 1):
+        sel = torch.randint(0, cnt, (min(batch, cnt),), generator=g).to(dev)
+        xb, tb = X[sel].contiguous(), T[sel].contiguous()
+        loss, G = grad(xb, tb, P)
+        rc = L.jk_mlp_adam(P.numel(), _vp(P), _vp(G), _vp(M), _vp(V), it, lr, 0.9, 0.999, 1e-8, st)
+        if rc < 0:
+            raise JkError(rc, "adam: ")
+        if it % 100 == 0 or it == iters:
+            hist.append((it, float(loss.item())))
+            if log:
+                log(it, hist[-1][1])
+    return P.cpu().numpy(), hist
+
+
+class Scorer:
+    """A trained network on the device (jk_scorer_create)."""
+
+    def __init__(self, params, stall_k=8):
+        p = np.ascontiguousarray(np.asarray(params, np.float32))
+        if p.size != nparams():
+            raise ValueError(f"expected {nparams()} parameters")
+        info = C.c_int(0)
+        self._s = lib().jk_scorer_create(NF, p.ctypes.data_as(C.POINTER(C.c_float)), int(stall_k), C.byref(info))
+        if not self._s:
+            raise JkError(info.value, "scorer: ")
+
+    def step_loop_dev(self, A, U, Z, sigma, J, n_2=0, stream=None, max_steps=0):
+        """jk_dstep_loop_dev_scored on column-major torch tensors; returns (INFO, exact steps)."""
+        import torch
+        n = A.shape[0]
+        for t in (A, U, Z):
+            assert t.is_cuda and t.dtype == torch.float64 and t.shape == (n, n) and t.stride() == (1, n)
+        Jc = np.ascontiguousarray(np.asarray(J).astype(np.int32))
+        o = _opts(max_steps, 0, 0, A.device.index or 0)
+        st = stream if stream is not None else torch.cuda.current_stream(A.device)
+        ex = C.c_int(0)
+        info = lib().jk_dstep_loop_dev_scored(n, U.data_ptr(), A.data_ptr(), Z.data_ptr(),
+                                              Jc.ctypes.data_as(C.POINTER(C.c_int)), sigma.data_ptr(), int(n_2), self._s,
+                                              C.byref(o), None, C.byref(ex), C.c_void_p(st.cuda_stream))
+        if info < 0 and info != -24:
+            raise JkError(info, "scored step loop: ")
+        return info, ex.value
+
+    def close(self):
+        if self._s:
+            lib().jk_scorer_destroy(self._s)
+            self._s = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+__all__ = ["NF", "nparams", "g_of", "init_params", "features", "forward", "grad", "training_data", "train", "Scorer",
+           "Opts"]
