@@ -59,6 +59,44 @@ def batch(count: int, nmin: int = 16, nmax: int = 128, seed: int = 4):
     return out
 
 
+def prescribed(sigma, J, seed: int = 6, rotations: int | None = None, t_max: float = 0.5) -> np.ndarray:
+    """A matrix with the prescribed hyperbolic singular values: Y = Q diag(sigma) H with Q
+    orthogonal (Haar) and H J-orthogonal (H^T J H = J), a product of random hyperbolic
+    rotations between a J = +1 and a J = -1 index (|tanh| <= tanh(t_max)) and plane rotations
+    within a sign class.  The hyperbolic singular values of Y are sigma, each attached to its
+    J entry, the known answer of the indefinite matrix Y J Y^T with eigenvalues J_i sigma_i^2
+    (the construction of the reference's data generator, src/var/old/jkdatgen/, from a
+    prescribed spectrum)."""
+    sigma = np.asarray(sigma, np.float64)
+    J = np.asarray(J)
+    n = sigma.size
+    r = _rng(seed)
+    Q, R = np.linalg.qr(r.standard_normal((n, n)))
+    Q *= np.sign(np.diag(R))
+    H = np.eye(n)
+    plus = np.nonzero(J == 1)[0]
+    minus = np.nonzero(J == -1)[0]
+    for _ in range(3 * n if rotations is None else rotations):
+        if plus.size and minus.size and r.uniform() < 0.5:
+            i, k = int(r.choice(plus)), int(r.choice(minus))
+            t = r.uniform(-t_max, t_max)
+            c, s = np.cosh(t), np.sinh(t)
+        else:
+            cls = plus if (plus.size > 1 and (minus.size < 2 or r.uniform() < 0.5)) else minus
+            if cls.size < 2:
+                continue
+            i, k = (int(x) for x in r.choice(cls, 2, replace=False))
+            t = r.uniform(0.0, 2.0 * np.pi)
+            c, s = np.cos(t), np.sin(t)
+            s = -s  # a plane rotation [[c, -s], [s, c]] on rows i, k
+            hi, hk = H[i].copy(), H[k].copy()
+            H[i], H[k] = c * hi + s * hk, -s * hi + c * hk
+            continue
+        hi, hk = H[i].copy(), H[k].copy()
+        H[i], H[k] = c * hi + s * hk, s * hi + c * hk
+    return np.asfortranarray(Q @ (sigma[:, None] * H))
+
+
 # The five workloads of the benchmark plan, by name.
 WORKLOADS = {
     "djk_n256": dict(kind="real", n=256, n_2=128, make=lambda: gaussian(256, seed=1, n_plus=192)),

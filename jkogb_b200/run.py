@@ -1,12 +1,16 @@
 """Run one named workload through the library on the current GPU.
 
   python -m jkogb_b200.run WORKLOAD [--max-steps S] [--weights R]
+  python -m jkogb_b200.run batch4096 [--matrices M] [--min-n K] [--max-steps S]
 
 Without --weights: one device-resident solve of the workload (jk_dstep_loop_dev /
 jk_zstep_loop_dev), stopped after S steps when --max-steps is given (the API's own step
 limit, INFO = -24), and prints INFO and the wall time.  With --weights R: R launches of
 one build's pair weights (jk_handle_weights) on the workload's input Y, the kernel-level
-form of the weight phase.  Both are the small, bounded invocations a profiler is pointed at.
+form of the weight phase.  For the batched workload: one launch of the batched solver
+(jk_dstep_loop_batched) over its first M matrices of order >= K (all by default), each
+stopped after S steps when given.  All are the small, bounded invocations a profiler is
+pointed at.
 """
 from __future__ import annotations
 
@@ -20,7 +24,9 @@ from . import gen
 
 def main(argv=None):
     ap = argparse.ArgumentParser(prog="python -m jkogb_b200.run")
-    ap.add_argument("workload", choices=sorted(gen.WORKLOADS))
+    ap.add_argument("workload", choices=sorted(gen.WORKLOADS) + ["batch4096"])
+    ap.add_argument("--matrices", type=int, default=0)
+    ap.add_argument("--min-n", type=int, default=0)
     ap.add_argument("--max-steps", type=int, default=0)
     ap.add_argument("--weights", type=int, default=0)
     a = ap.parse_args(argv)
@@ -29,6 +35,15 @@ def main(argv=None):
 
     import jkogb_b200 as jk
 
+    if a.workload == "batch4096":
+        b = [x for x in gen.batch(4096, 16, 128, seed=4) if x[0].shape[0] >= a.min_n]
+        if a.matrices > 0:
+            b = b[:a.matrices]
+        t0 = time.perf_counter()
+        res = jk.dstep_loop_batched([x[0] for x in b], [x[1] for x in b], max_steps=a.max_steps)
+        info = np.array([r["info"] for r in res])
+        print(f"batch4096: {len(b)} matrices in {time.perf_counter() - t0:.3f} s, INFO min {info.min()} max {info.max()}")
+        return 0
     wl = gen.WORKLOADS[a.workload]
     Y, J = wl["make"]()
     n, n_2 = wl["n"], wl["n_2"]
