@@ -224,29 +224,12 @@ __device__ __forceinline__ bool hyp_pair_setup(const double *__restrict__ A, int
                    a_is_p ? 1 : -1, w, d, t);
 }
 
-// The real hyperbolic weights in two kernels.  k_hyp_setup (one thread per pair)
-// runs the 2x2 HSVD of DMAGF2H and either writes the weight (no scan needed) or the
-// scan parameters of the pair; k_hyp_scan streams row chunks of 16 "+" x 16 PPT "-"
-// columns through a double buffer in shared memory (cp.async) and runs the
-// sequential ABODNDF2 fma chains, PPT pairs per thread sharing its "+" column.
-// Index-range tiles: tile (tp, tq), tp <= tq, holds the pairs p in [32 tp, 32 tp + 32),
-// q in [32 tq, 32 tq + 32), p < q, J(p) != J(q).  k_hyp_tile lists a tile's pairs,
-// runs their 2x2 HSVDs and either stores the weight (no scan) or the scan
-// parameters, then stages the tile's two column ranges in row chunks and runs the
-// fma chains.  Rows p and q can only lie in the two ranges, so the chunks outside
-// them run without a per-row skip test.
+// The real hyperbolic weights, pipelined (k_hyp_pm below): sign-class tiles of 32 "+"
+// by 32 "-" vertices, 64 rows per chunk staged with cp.async, the sequential ABODNDF2
+// fma chains of four pairs per thread.
 #define TW 32
 #define SCAN_ROWS 64
 #define SCAN_RS (SCAN_ROWS + 2)
-
-__device__ __forceinline__ void tile_of(int b, int T, int &tp, int &tq)
-{
-  // b enumerates the tiles row by row of the upper triangle
-  int r = 0;
-  while (b >= T - r) { b -= T - r; ++r; }
-  tp = r;
-  tq = r + b;
-}
 
 // K pairs per thread (slots t, t + 256, ...); FAST: no row of this chunk is a p or q
 template <int K, bool FAST>
@@ -282,28 +265,35 @@ __device__ __forceinline__ void scan_chunk(const double *const *xs, const double
 #define SCAN_THREADS 256
 #define SCAN_STAGES 3
 
-// one tile: list its pairs and run their 2x2 HSVDs (k_hyp_setup's work, parameters
-// to this tile's slice of `par`), then stream the two column ranges through a
-// three-stage buffer and run the fma chains, up to 4 pairs per thread
+// one sign-class tile: tile (ti, tj) holds the pairs of the "+" vertices
+// plus[32 ti .. 32 ti + 31] with the "-" vertices minus[32 tj .. 32 tj + 31], all of
+// them hyperbolic (up to 1024, 4 per thread).  First the 2x2 HSVDs of DMAGF2H (scan
+// parameters to this tile's slice of `par`, the other weights straight to W), then the
+// tile's 64 columns stream through a three-stage buffer in row chunks and every thread
+// runs its pairs' fma chains.  A warp whose pairs have none of their rows p, q in a
+// chunk runs that chunk without the per-row skip test.
 __global__ void __launch_bounds__(SCAN_THREADS, 2)
-k_hyp_tile(const State *st, const double *__restrict__ A, const int *__restrict__ J, int n, double *__restrict__ Wm,
-           HypPar *par)
+k_hyp_pm(const State *st, const double *__restrict__ A, const int *__restrict__ plus, const int *__restrict__ minus,
+         int n_plus, int n_minus, int n, double *__restrict__ Wm, HypPar *par)
 {
   if (st->stop || st->learned_step) return;  // a learned step ranks these pairs by the scorer
-  const int T = (n + TW - 1) / TW;
-  int tp, tq;
-  tile_of(blockIdx.x, T, tp, tq);
-  const int P0 = tp * TW, Q0 = tq * TW;
+  const int TM = (n_minus + TW - 1) / TW;
+  const int P0 = (blockIdx.x / TM) * TW, Q0 = (blockIdx.x % TM) * TW;
   HypPar *tpar = par + (long long)blockIdx.x * (TW * TW);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  __shared__ int s_cnt, s_warp[SCAN_THREADS / 32];
+  __shared__ int s_cnt, s_warp[SCAN_THREADS / 32], s_col[2 * TW];
+  if (tid < 2 * TW) {
+    const int c = tid;
+    s_col[c] = (c < TW) ? ((P0 + c < n_plus) ? plus[P0 + c] : -1) : ((Q0 + c - TW < n_minus) ? minus[Q0 + c - TW] : -1);
+  }
   if (tid == 0) s_cnt = 0;
   __syncthreads();
   for (int base = 0; base < TW * TW; base += SCAN_THREADS) {
     const int l = base + tid;
-    const int p = P0 + l / TW, q = Q0 + l % TW;
-    const bool hyp = (p < n) && (q < n) && (p < q) && (J[p] != J[q]);
-    const unsigned m = __ballot_sync(0xFFFFFFFFu, hyp);
+    const int ci = l / TW, cj = TW + l % TW;  // tile columns of the "+" and the "-" vertex
+    const int a = s_col[ci], b = s_col[cj];
+    const bool valid = (a >= 0) && (b >= 0);
+    const unsigned m = __ballot_sync(0xFFFFFFFFu, valid);
     if (!lane) s_warp[warp] = __popc(m);
     __syncthreads();
     int off = s_cnt;
@@ -311,15 +301,15 @@ k_hyp_tile(const State *st, const double *__restrict__ A, const int *__restrict_
     const int slot = off + __popc(m & ((1u << lane) - 1u));
     __syncthreads();
     if (tid == 0) { int t = 0; for (int w2 = 0; w2 < SCAN_THREADS / 32; ++w2) t += s_warp[w2]; s_cnt += t; }
-    if (hyp) {
+    if (valid) {
       int pp, qq;
       bool ap;
       double w, d0 = 0.0;
       Rot t;
-      const int a = (J[p] == 1) ? p : q, bcol = (J[p] == 1) ? q : p;  // the "+" column first
-      const bool sc = hyp_pair_setup(A, n, a, bcol, pp, qq, ap, w, d0, t);
+      const bool sc = hyp_pair_setup(A, n, a, b, pp, qq, ap, w, d0, t);
       HypPar h;
-      h.p = pp; h.q = qq; h.pad = 0;
+      h.p = pp; h.q = qq;
+      h.pad = ap ? (ci | (cj << 8)) : (cj | (ci << 8));  // the tile columns of p and of q
       h.flags = sc ? (1 | (t.c1 ? 2 : 0) | (t.c2 ? 4 : 0)) : 0;
       h.r1 = sc ? t.r1 : 0.0; h.r2 = sc ? t.r2 : 0.0; h.m1 = sc ? t.m1 : 0.0; h.m2 = sc ? t.m2 : 0.0;
       h.d = d0;
@@ -336,18 +326,18 @@ k_hyp_tile(const State *st, const double *__restrict__ A, const int *__restrict_
   if (!cnt) return;
 
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  double *buf = (double *)smem_raw;  // [SCAN_STAGES][2 * TW][SCAN_RS]: columns P0.., then Q0..
+  double *buf = (double *)smem_raw;  // [SCAN_STAGES][2 * TW][SCAN_RS]: the "+" columns, then the "-" columns
   constexpr int K = 4, STAGE = 2 * TW * SCAN_RS;
-  int pl[K], ql[K], fl[K];
+  int pv[K], qv[K], cpq[K], fl[K];  // cpq: the tile columns of p (bits 0-7) and q (bits 8-15)
   double r1[K], r2[K], m1[K], m2[K], d[K];
   int kw = 0;  // active slots of this warp (warp-uniform)
 #pragma unroll
   for (int k = 0; k < K; ++k) {
     const int slot = tid + SCAN_THREADS * k;
-    fl[k] = 0; pl[k] = ql[k] = 0; r1[k] = r2[k] = m1[k] = m2[k] = d[k] = 0.0;
+    fl[k] = 0; pv[k] = qv[k] = -1; cpq[k] = 0; r1[k] = r2[k] = m1[k] = m2[k] = d[k] = 0.0;
     if (slot < cnt) {
       const HypPar h = tpar[slot];
-      fl[k] = h.flags; pl[k] = h.p - P0; ql[k] = h.q - Q0; d[k] = h.d;
+      fl[k] = h.flags; pv[k] = h.p; qv[k] = h.q; cpq[k] = h.pad; d[k] = h.d;
       r1[k] = h.r1; r2[k] = h.r2; m1[k] = h.m1; m2[k] = h.m2;
     }
     if (SCAN_THREADS * k + 32 * warp < cnt) kw = k + 1;
@@ -369,8 +359,8 @@ k_hyp_tile(const State *st, const double *__restrict__ A, const int *__restrict_
 #pragma unroll
         for (int j = 0; j < 16; ++j) {
           const int col = sc0 + 4 * j;
-          const int g = (col < TW) ? (P0 + col) : (Q0 + col - TW);
-          if (g < n) cp_async8(dst + col * SCAN_RS + sr, A + (long long)g * n + i0 + sr);
+          const int g = s_col[col];
+          if (g >= 0) cp_async8(dst + col * SCAN_RS + sr, A + (long long)g * n + i0 + sr);
         }
       }
     }
@@ -386,14 +376,16 @@ k_hyp_tile(const State *st, const double *__restrict__ A, const int *__restrict_
     const int i0 = c * SCAN_ROWS, rows = min(SCAN_ROWS, n - i0);
     const double *xs[K], *ys[K];
     int pr[K], qr[K];
+    bool mine = false;
 #pragma unroll
     for (int k = 0; k < K; ++k) {
-      xs[k] = bb + pl[k] * SCAN_RS;
-      ys[k] = bb + (TW + ql[k]) * SCAN_RS;
-      pr[k] = pl[k] + P0 - i0;  // p, q as rows of this chunk
-      qr[k] = ql[k] + Q0 - i0;
+      xs[k] = bb + (cpq[k] & 0xFF) * SCAN_RS;
+      ys[k] = bb + ((cpq[k] >> 8) & 0xFF) * SCAN_RS;
+      pr[k] = pv[k] - i0;  // p, q as rows of this chunk
+      qr[k] = qv[k] - i0;
+      if (fl[k] & 1) mine = mine || (pr[k] >= 0 && pr[k] < rows) || (qr[k] >= 0 && qr[k] < rows);
     }
-    const bool touch = (i0 < P0 + TW && P0 < i0 + rows) || (i0 < Q0 + TW && Q0 < i0 + rows);
+    const bool touch = __any_sync(0xFFFFFFFFu, mine);
     if (allfast) {
       if (!touch) {
         if (kw == 4) scan_chunk<4, true>(xs, ys, pr, qr, fl, r1, r2, m1, m2, d, rows);
@@ -415,7 +407,7 @@ k_hyp_tile(const State *st, const double *__restrict__ A, const int *__restrict_
           Rot t;
           t.c1 = (fl[k] >> 1) & 1; t.c2 = (fl[k] >> 2) & 1;
           t.r1 = r1[k]; t.r2 = r2[k]; t.m1 = m1[k]; t.m2 = m2[k];
-          scan_rows_real(xs[k], ys[k], rows, i0, pl[k] + P0, ql[k] + Q0, t, d[k]);
+          scan_rows_real(xs[k], ys[k], rows, i0, pv[k], qv[k], t, d[k]);
         }
     }
   }
@@ -423,7 +415,7 @@ k_hyp_tile(const State *st, const double *__restrict__ A, const int *__restrict_
 #pragma unroll
   for (int k = 0; k < K; ++k) {
     if (!(fl[k] & 1)) continue;
-    const int p = pl[k] + P0, q = ql[k] + Q0;
+    const int p = pv[k], q = qv[k];
     double x = d[k];
     if (x < -JK_HUGE) x = nan_w();
     Wm[(long long)q * n + p] = x;
@@ -1069,7 +1061,7 @@ cudaError_t prepare_kernels(int n)
   // block, the ranking and matching state of k_select
   cudaError_t e = cudaFuncSetAttribute(k_rotate<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * n * 8);
   if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(k_hyp_tile, cudaFuncAttributeMaxDynamicSharedMemorySize, SCAN_STAGES * (2 * TW) * SCAN_RS * (int)sizeof(double));
+    e = cudaFuncSetAttribute(k_hyp_pm, cudaFuncAttributeMaxDynamicSharedMemorySize, SCAN_STAGES * (2 * TW) * SCAN_RS * (int)sizeof(double));
   if (e == cudaSuccess) e = cudaFuncSetAttribute(k_rotate<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * n * 16);
   const int ss = (int)select_smem(n);
   if (e == cudaSuccess) e = cudaFuncSetAttribute(k_select<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, ss);
@@ -1092,9 +1084,11 @@ cudaError_t launch_init(Workspace &w, void *U, void *Z, cudaStream_t s)
 
 static void hyp_d_launch(Workspace &w, const double *A, cudaStream_t s)
 {
-  const int T = (w.n + TW - 1) / TW, nt = T * (T + 1) / 2;
+  // ceil(n_plus / 32) ceil(n_minus / 32) <= T (T + 1) / 2 tiles, T = ceil(n / 32): the
+  // parameter slices make_workspace allocates
+  const int nt = ((w.n_plus + TW - 1) / TW) * ((w.n_minus + TW - 1) / TW);
   const size_t smem = SCAN_STAGES * (2 * TW) * SCAN_RS * sizeof(double);
-  k_hyp_tile<<<nt, SCAN_THREADS, smem, s>>>(w.st, A, w.J, w.n, w.Wm, (HypPar *)w.hpar);
+  k_hyp_pm<<<nt, SCAN_THREADS, smem, s>>>(w.st, A, w.plus, w.minus, w.n_plus, w.n_minus, w.n, w.Wm, (HypPar *)w.hpar);
 }
 
 template <typename T>
