@@ -430,7 +430,7 @@ def run_ours(args, wl):
         "gpu_launches": launches,
         "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                      "frac": achieved / peak if peak > 0 else None, "traffic": traffic,
-                     "kernel": "pair weights (k_weights_trig + k_hyp_tile), timed alone on the input Y",
+                     "kernel": "pair weights (k_weights_trig + k_hyp_pm), timed alone on the input Y",
                      "algorithmic_flop_per_launch": flops, "launch_ms": w_ms,
                      "peak_note": "FP64 FMA throughput measured live by jk_fp64_peak; the weight scan's op mix "
                                   "(4 fma, 2 mul, 4 add per 14 flop) bounds it at 0.70 of that peak"},
