@@ -7,8 +7,10 @@
  *     src/D/dstep.F90:472-604, called from src/D/djk.F90:253
  *   ZSTEP_LOOP(...)  src/Z/zstep.F90:482-615, called from src/Z/zjk.F90
  * together with the strategy plug-ins DPROC_INIT selects (src/D/dstep.F90:76-134):
- * ID_NCP 0/1/2 (greedy non-colliding selection, AW_NCP1 == AW_NCP2) and ID_TRU 0/1/2
- * (pair enumeration; the selection is a total order, so it does not change results).
+ * ID_NCP 0/1/2 (greedy non-colliding selection, AW_NCP1 == AW_NCP2), 3 (AW_NCP3, the best
+ * of the greedy walks from every start offset, src/shared/atypes.F90:488-592; its work
+ * grows as N^4 per step, so N <= 256) and ID_TRU 0/1/2 (pair enumeration; the
+ * selection is a total order, so it does not change results).
  * The caller's workspaces of the Fortran interface (NN, P, Q, NM, DZ, STEP, TT, W) live
  * on the device and are not arguments here.
  *
@@ -52,8 +54,8 @@ typedef struct {
 
 #define JK_ERR_CUDA (-30)       /* a CUDA runtime error */
 #define JK_ERR_NOMEM (-31)      /* device allocation failed */
-#define JK_ERR_TOO_LARGE (-32)  /* N beyond this build's limit (see jk_max_order) */
-#define JK_ERR_ID_NCP (-21)     /* ID_NCP outside 0..2 */
+#define JK_ERR_TOO_LARGE (-32)  /* N beyond this build's limit (see jk_max_order; 256 for ID_NCP = 3) */
+#define JK_ERR_ID_NCP (-21)     /* ID_NCP outside 0..3 */
 #define JK_ERR_ID_TRU (-22)     /* ID_TRU outside 0..2 */
 #define JK_ERR_J (-23)          /* a J entry is not +1 or -1 (TRU1/TRU2, src/shared/jstep.F90:38-39) */
 #define JK_ERR_MAX_STEPS (-24)  /* opts->max_steps reached */

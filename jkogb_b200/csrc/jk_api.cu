@@ -60,7 +60,8 @@ int check_args(int n, int ldu, int lda, int ldz, const int *J, int n_2, int id_n
   if (lda < n) return -5;
   if (ldz < n) return -7;
   if (n_2 < 0) return -16;
-  if (id_ncp < 0 || id_ncp > 2) return JK_ERR_ID_NCP;
+  if (id_ncp < 0 || id_ncp > 3) return JK_ERR_ID_NCP;
+  if (id_ncp == 3 && n > kNcp3MaxN) return JK_ERR_TOO_LARGE;
   if (id_tru < 0 || id_tru > 2) return JK_ERR_ID_TRU;
   if (!J) return -8;
   for (int i = 0; i < n; ++i)
@@ -152,8 +153,7 @@ namespace {
 int run_loop(int cplx, int n, void *dU, void *dA, void *dZ, const int *J, double *dsigma, int n_2, int id_ncp, int id_tru,
              const jk_opts *opts, jk_trace *trace, cudaStream_t s, const jk_scorer *sc = nullptr, int *exact_steps = nullptr)
 {
-  (void)id_ncp;
-  (void)id_tru;
+  (void)id_tru;  // the pair order does not change the sorted records
   jk_opts o;
   memset(&o, 0, sizeof(o));
   if (opts) o = *opts;
@@ -164,6 +164,17 @@ int run_loop(int cplx, int n, void *dU, void *dA, void *dZ, const int *J, double
   int rc = make_workspace(g, w, n, cplx, J, trace_on, trace ? trace->max_steps : 0, trace ? trace->max_piv : 0);
   if (rc) return rc;
   w.zba_quirk = (o.zba_quirk == 0) ? 1 : 0;
+  w.id_ncp = id_ncp;
+  if (id_ncp == 3) {
+    const size_t nn = (size_t)n * (n - 1) / 2;
+    CK(g.alloc(&w.n3key, nn * sizeof(unsigned long long)));
+    CK(g.alloc(&w.n3tie, nn * sizeof(unsigned)));
+    CK(g.alloc(&w.n3sorted, nn * sizeof(int)));
+    CK(g.alloc(&w.n3val, nn * sizeof(double)));
+    CK(g.alloc(&w.n3len, nn * sizeof(int)));
+    CK(g.alloc(&w.n3it, sizeof(int)));
+    CK(cudaMemset(w.n3it, 0, sizeof(int)));
+  }
   if (sc) {
     // a learned solve: the scorer's device parameters, the off-norm buffers, the mode flags
     w.learned = 1;
@@ -773,7 +784,7 @@ const char *jk_strerror(int info)
   case -16: return "N_2 < 0";
   case -10: return "a 2x2 hyperbolic transformation with |tanh| >= 1 (KHSVD2U)";
   case -11: return "a 2x2 hyperbolic transformation with |tanh| >= 1 (KHSVD2L)";
-  case JK_ERR_ID_NCP: return "ID_NCP not in 0..2";
+  case JK_ERR_ID_NCP: return "ID_NCP not in 0..3";
   case JK_ERR_ID_TRU: return "ID_TRU not in 0..2";
   case JK_ERR_J: return "a J entry is neither +1 nor -1";
   case JK_ERR_MAX_STEPS: return "the step limit was reached";

@@ -110,7 +110,7 @@ int main(int argc, char **argv)
   if (n <= 2) stop("N should be at least 3 (for N=2 use dtest)");
   n_2 = jstep_len(n, n_2);
   if (n_2 <= 0) stop("JSTEP_LEN");
-  if (id_ncp < 0 || id_ncp > 2 || id_tru < 0 || id_tru > 2) stop("DPROC_INIT");
+  if (id_ncp < 0 || id_ncp > 3 || id_tru < 0 || id_tru > 2) stop("DPROC_INIT");
 
   const size_t nn = (size_t)n * n;
   std::vector<double> A;

@@ -98,7 +98,14 @@ struct Workspace {
   int *offcount;     // blocks done (the last one finishes the off-norm)
   int learned;       // rank the scanned hyperbolic pairs by `sc`
   ScorerDev sc;
+  // ID_NCP = 3 (AW_NCP3): per record key and tie, the sorted order, every start's walk
+  int id_ncp;
+  unsigned long long *n3key;
+  unsigned *n3tie;
+  int *n3sorted, *n3len, *n3it;
+  double *n3val;
 };
+constexpr int kNcp3MaxN = 256;  // AW_NCP3's work grows as the square of the record count
 
 // host launchers (jk_kernels.cu)
 cudaError_t launch_init(Workspace &w, void *U, void *Z, cudaStream_t s);

@@ -919,6 +919,201 @@ __global__ void k_pivots(State *st, const T *__restrict__ A, const int *__restri
   rr[r] = x;
 }
 
+// ---------------------------------------------------------------------------
+// ID_NCP = 3: AW_NCP3 (src/shared/atypes.F90:488-592), the best of the greedy walks
+// that start at every position of the sorted record list.  For every start offset
+// I = 1..IT, AW_NCP2 walks the records I..IT and takes every record whose P and Q
+// are both unused, up to N_2; the walk's value is (sum of its weights up to its last
+// positive one, added from that one back to the first) + (the sum of the rest, in
+// order).  The walk with the largest value wins, ties to the smaller start.  The
+// work grows as IT^2, so this strategy is limited to small orders (kNcp3MaxN).
+//   k_ncp3_keys    one record per pair: the order key (weight, band, p), NaN last
+//   k_ncp3_rank    every record's position by counting the records ahead of it
+//   k_ncp3_walks   one warp per start offset: the walk, its length and value
+//   k_ncp3_pick    one block: the end of the previous step, the best walk again as
+//                  this step's pivots, the columns outside them
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int ncp3_tri(int p, int q) { return (q * (q - 1)) / 2 + p; }
+
+__global__ void k_ncp3_keys(const State *st, const double *__restrict__ Wm, int n, unsigned long long *key, unsigned *tie,
+                            int *it)
+{
+  if (st->stop) return;
+  const int p = blockIdx.x * 32 + threadIdx.x, q = blockIdx.y * 8 + threadIdx.y;
+  if (p >= n || q >= n || p >= q) return;
+  const int k = ncp3_tri(p, q);
+  const unsigned long long kk = wkey(Wm[(long long)q * n + p]);
+  key[k] = kk;
+  tie[k] = tkey(p, q);
+  if (kk) atomicAdd(it, 1);
+}
+
+__global__ void k_ncp3_rank(const State *st, const unsigned long long *__restrict__ key, const unsigned *__restrict__ tie,
+                            int nn, int *sorted)
+{
+  if (st->stop) return;
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= nn) return;
+  const unsigned long long kr = key[r];
+  const unsigned tr = tie[r];
+  int rank = 0;
+  for (int o = 0; o < nn; ++o) rank += kbetter(key[o], tie[o], kr, tr) ? 1 : 0;
+  sorted[rank] = r;
+}
+
+// the walk from start offset i (0-based) by one warp: picks (p, q) in order into
+// pk/qk (when not NULL) and their weights into wv; returns the number of picks
+__device__ int ncp3_walk(int i, int it, int n, int n_2, const int *__restrict__ sorted, const unsigned *__restrict__ tie,
+                         const double *__restrict__ Wm, unsigned *used, double *wv, int *pk, int *qk)
+{
+  const int lane = threadIdx.x & 31;
+  for (int k = lane; k < (n + 31) / 32; k += 32) used[k] = 0u;
+  __syncwarp();
+  int picks = 0;
+  for (int base = i; base < it && picks < n_2; base += 32) {
+    const int idx = base + lane;
+    int p = -1, q = -1;
+    bool valid = false;
+    if (idx < it) {
+      const unsigned t = tie[sorted[idx]];
+      p = (int)(t & 0xFFFFu);
+      q = p + (int)(t >> 16);
+      valid = !((used[p >> 5] >> (p & 31)) & 1u) && !((used[q >> 5] >> (q & 31)) & 1u);
+    }
+    unsigned cand = __ballot_sync(0xFFFFFFFFu, valid);
+    while (cand && picks < n_2) {
+      const int k = __ffs(cand) - 1;
+      const int p1 = __shfl_sync(0xFFFFFFFFu, p, k), q1 = __shfl_sync(0xFFFFFFFFu, q, k);
+      if (lane == 0) {
+        used[p1 >> 5] |= 1u << (p1 & 31);
+        used[q1 >> 5] |= 1u << (q1 & 31);
+        wv[picks] = Wm[(long long)q1 * n + p1];
+        if (pk) { pk[picks] = p1; qk[picks] = q1; }
+      }
+      ++picks;
+      valid = valid && (lane > k) && p != p1 && p != q1 && q != p1 && q != q1;
+      cand = __ballot_sync(0xFFFFFFFFu, valid);
+    }
+    __syncwarp();
+  }
+  __syncwarp();
+  return picks;
+}
+
+// the value of a walk (AW_NCP3's MYWP + MYWN)
+__device__ double ncp3_value(const double *wv, int sl)
+{
+  int l = 0;
+  for (int k = sl; k >= 1; --k)
+    if (wv[k - 1] > 0.0) { l = k; break; }
+  double wp = 0.0, wn = 0.0;
+  for (int k = l; k >= 1; --k) wp = __dadd_rn(wp, wv[k - 1]);
+  for (int k = l + 1; k <= sl; ++k) wn = __dadd_rn(wn, wv[k - 1]);
+  return __dadd_rn(wp, wn);
+}
+
+#define NCP3_WARPS 8
+
+__global__ void __launch_bounds__(NCP3_WARPS * 32)
+k_ncp3_walks(const State *st, const int *__restrict__ itp, const int *__restrict__ sorted, const unsigned *__restrict__ tie,
+             const double *__restrict__ Wm, int n, int n_2, double *val, int *len)
+{
+  if (st->stop) return;
+  __shared__ unsigned used[NCP3_WARPS][kNcp3MaxN / 32];
+  __shared__ double wv[NCP3_WARPS][kNcp3MaxN / 2];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int i = blockIdx.x * NCP3_WARPS + warp, it = *itp;
+  if (i >= it) return;
+  const int sl = ncp3_walk(i, it, n, n_2, sorted, tie, Wm, used[warp], wv[warp], nullptr, nullptr);
+  if (lane == 0) {
+    val[i] = ncp3_value(wv[warp], sl);
+    len[i] = sl;
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256)
+k_ncp3_pick(State *st, const int *__restrict__ itp, const int *__restrict__ sorted, const unsigned *__restrict__ tie,
+            const double *__restrict__ Wm, const int *__restrict__ J, int n, int n_2, const double *__restrict__ val,
+            Piv<T> *piv, int *unp, int *itc, Trace tr)
+{
+  __shared__ int s_stop, s_best, s_sl, s_nunp;
+  __shared__ double bv[256];
+  __shared__ int bi[256];
+  __shared__ unsigned used[kNcp3MaxN / 32];
+  __shared__ double wv[kNcp3MaxN / 2];
+  __shared__ int pk[kNcp3MaxN / 2], qk[kNcp3MaxN / 2];
+  __shared__ unsigned char ms[kNcp3MaxN];
+  const int tid = threadIdx.x;
+  if (tid == 0) {
+    end_of_step<T>(st, piv, J, tr);
+    s_stop = st->stop;
+    s_nunp = 0;
+  }
+  __syncthreads();
+  const int it = *itp;
+  if (s_stop) {
+    if (tid == 0) *itc = 0;
+    return;
+  }
+  // the best walk: the largest value, ties to the smaller start
+  double b = 0.0;
+  int bj = -1;
+  for (int i = tid; i < it; i += blockDim.x) {
+    const double v = val[i];
+    if (bj < 0 || !(v <= b)) { b = v; bj = i; }
+  }
+  bv[tid] = b;
+  bi[tid] = bj;
+  __syncthreads();
+  if (tid == 0) {
+    double bb = 0.0;
+    int bb_i = -1;
+    for (int t = 0; t < (int)blockDim.x; ++t) {
+      if (bi[t] < 0) continue;
+      if (bb_i < 0 || !(bv[t] <= bb) || (bv[t] == bb && bi[t] < bb_i)) { bb = bv[t]; bb_i = bi[t]; }
+    }
+    s_best = bb_i;
+  }
+  __syncthreads();
+  if (tid < 32) {
+    const int sl = (s_best >= 0) ? ncp3_walk(s_best, it, n, n_2, sorted, tie, Wm, used, wv, pk, qk) : 0;
+    if (tid == 0) s_sl = sl;
+  }
+  for (int v = tid; v < n; v += blockDim.x) ms[v] = 0;
+  __syncthreads();
+  const int sl = s_sl;
+  for (int r = tid; r < sl; r += blockDim.x) {
+    ms[pk[r]] = 1;
+    ms[qk[r]] = 1;
+    Piv<T> &pv = piv[r];
+    pv.p = pk[r];
+    pv.q = qk[r];
+    pv.w = wv[r];
+  }
+  __syncthreads();
+  for (int v = tid; v < n; v += blockDim.x)
+    if (!ms[v]) unp[atomicAdd(&s_nunp, 1)] = v;
+  __syncthreads();
+  if (tid == 0) {
+    *itc = 0;  // the record count of the next step starts from zero
+    st->sl = sl;
+    st->nl = 0;
+    st->err = 0;
+    st->nunp = s_nunp;
+    st->rounds = it;
+    if (sl <= 0) {
+      st->info = st->steps;
+      st->stop = 1;
+      if (st->trace_on && st->trace_steps < st->trace_cap_steps) {
+        const int s = st->trace_steps++;
+        tr.sl[s] = 0; tr.nl[s] = -1; tr.tw[s] = -0.0; tr.trig[s] = 0; tr.hyp[s] = 0; tr.rounds[s] = it;
+      }
+    }
+    else st->pending = 1;
+  }
+}
+
 size_t select_smem(int n)
 {
   const int s2 = pow2ceil(n / 2 > 0 ? n / 2 : 1);
@@ -1137,9 +1332,22 @@ template <typename T>
 static cudaError_t select_t(Workspace &w, const T *A, int n_2, cudaStream_t s)
 {
   const int n = w.n;
-  cudaError_t e = colsort(w, s);
-  if (e != cudaSuccess) return e;
-  k_select<T><<<1, SEL_THREADS, select_smem(n), s>>>(w.st, w.Wm, w.J, n, n_2, w.list, w.len, (Piv<T> *)w.piv, w.unp, w.tr);
+  cudaError_t e = cudaSuccess;
+  if (w.id_ncp == 3) {
+    // AW_NCP3: every start offset's walk, then the best one
+    const int nn = n * (n - 1) / 2;
+    k_ncp3_keys<<<dim3((n + 31) / 32, (n + 7) / 8), dim3(32, 8), 0, s>>>(w.st, w.Wm, n, w.n3key, w.n3tie, w.n3it);
+    k_ncp3_rank<<<(nn + 255) / 256, 256, 0, s>>>(w.st, w.n3key, w.n3tie, nn, w.n3sorted);
+    k_ncp3_walks<<<(nn + NCP3_WARPS - 1) / NCP3_WARPS, NCP3_WARPS * 32, 0, s>>>(w.st, w.n3it, w.n3sorted, w.n3tie, w.Wm, n,
+                                                                                 n_2, w.n3val, w.n3len);
+    k_ncp3_pick<T><<<1, 256, 0, s>>>(w.st, w.n3it, w.n3sorted, w.n3tie, w.Wm, w.J, n, n_2, w.n3val, (Piv<T> *)w.piv, w.unp,
+                                     w.n3it, w.tr);
+  }
+  else {
+    e = colsort(w, s);
+    if (e != cudaSuccess) return e;
+    k_select<T><<<1, SEL_THREADS, select_smem(n), s>>>(w.st, w.Wm, w.J, n, n_2, w.list, w.len, (Piv<T> *)w.piv, w.unp, w.tr);
+  }
   if (A) {
     const int half = n / 2 > 0 ? n / 2 : 1;
     k_pivots<T><<<(half + 127) / 128, 128, 0, s>>>(w.st, A, w.J, n, (Piv<T> *)w.piv, (RowRot<T> *)w.rowrot, w.zba_quirk);

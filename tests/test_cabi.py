@@ -88,3 +88,17 @@ def test_batched_argument_errors_without_gpu():
     assert info.value == -23
     assert not L.jk_batch_create(0, ip(n), ip(n2), ip(J), None, ctypes.byref(info))
     assert info.value == -1
+
+
+def test_ncp3_order_limit_without_gpu():
+    # AW_NCP3 is limited to N <= 256; the check runs before any CUDA call
+    import numpy as np
+    import jkogb_b200 as jk
+    L = jk.lib()
+    n = 257
+    A = np.zeros((n, n))
+    J = np.ones(n, np.int32)
+    o = jk.Opts()
+    d = lambda a: a.ctypes.data  # noqa: E731
+    Jp = J.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+    assert L.jk_dstep_loop(n, d(A), n, d(A), n, d(A), n, Jp, d(A), 0, 3, 0, ctypes.byref(o), None) == -32
