@@ -52,6 +52,22 @@ def _dist():
     return ws, rank, local
 
 
+def max_over_ranks(x, device=None):
+    """The maximum of a per-rank number over all ranks: a multi-rank job takes as long as
+    its slowest rank.  Without an initialised process group of more than one rank, x."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    if dist.is_available() and dist.is_initialized() and dist.get_world_size() > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def rank_batch_seed(rank):
+    """The batched workload's seed on a rank: every rank solves its own 4096-matrix batch."""
+    return 4 + int(rank)
+
+
 def _clock_sampler(dev):
     f = open(os.path.join(ROOT, "gpurun_out" if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else ".",
                           f".clocks_{os.getpid()}.csv"), "w")
@@ -223,7 +239,7 @@ def run_ours_batch(args, wl):
         dist.init_process_group("nccl", timeout=timedelta(seconds=900), device_id=torch.device("cuda", local))
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
-    b = wl["make"](seed=4 + rank)  # one batch per rank: the ranks partition the job, no collective on the data path
+    b = wl["make"](seed=rank_batch_seed(rank))  # one batch per rank: no collective on the data path
     mats = [Y for Y, _ in b]
     Js = [J for _, J in b]
     A, J, n, off = jk.batch_pack(mats, Js)
@@ -265,10 +281,7 @@ def run_ours_batch(args, wl):
     barrier()
     clocks = _clock_summary(smi, smf)
     dev_ms = sum(a.elapsed_time(b) for a, b in ev)
-    t = torch.tensor([dev_ms], dtype=torch.float64, device=dev)
-    if ws > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms = float(t.item()) / args.steps
+    ms = max_over_ranks(dev_ms, dev) / args.steps
     info = di.cpu().numpy()
     plan.close()
 
@@ -278,10 +291,7 @@ def run_ours_batch(args, wl):
     for _ in range(args.steps):
         res = jk.dstep_loop_batched(mats, Js)
     e2e_s = (time.perf_counter() - tt0) / args.steps
-    te = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
-    if ws > 1:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_s = float(te.item())
+    e2e_s = max_over_ranks(e2e_s, dev)
     same = bool(np.array_equal(np.array([r["info"] for r in res]), info))
 
     # FP64 work of the weight scans of the whole batch: sum over matrices and steps of
@@ -371,10 +381,7 @@ def run_ours(args, wl):
     barrier()
     clocks = _clock_summary(smi, smf)
     dev_ms = e0.elapsed_time(e1)
-    t = torch.tensor([dev_ms], dtype=torch.float64, device=dev)
-    if ws > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_per_solve = float(t.item()) / args.steps
+    ms_per_solve = max_over_ranks(dev_ms, dev) / args.steps
 
     # end to end: the host-pointer C ABI (H2D of Y, D2H of U, Z, SIGMA inside the call)
     Yh = np.asfortranarray(Y)
@@ -383,10 +390,7 @@ def run_ours(args, wl):
     for _ in range(args.steps):
         r = jk.step_loop(Yh, J, n_2=n_2)
     e2e_s = (time.perf_counter() - tt0) / args.steps
-    te = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
-    if ws > 1:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_s = float(te.item())
+    e2e_s = max_over_ranks(e2e_s, dev)
     ok = bool(r["info"] == info)
 
     # the dominant kernel (the pair weights) timed alone on the workload's input
