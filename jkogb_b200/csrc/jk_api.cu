@@ -98,6 +98,7 @@ int make_workspace(Guard &g, Workspace &w, int n, int cplx, const int *J, int tr
   CK(g.alloc(&w.plus, (plus.size() + 1) * sizeof(int)));
   CK(g.alloc(&w.minus, (minus.size() + 1) * sizeof(int)));
   CK(g.alloc(&w.Wm, (size_t)n * n * sizeof(double)));
+  if (cplx) CK(g.alloc(&w.mag, (size_t)n * n * sizeof(double)));
   {
     const size_t T = (n + 31) / 32, nt = T * (T + 1) / 2;
     CK(g.alloc(&w.hpar, nt * 1024 * sizeof(HypPar)));
@@ -230,6 +231,7 @@ int run_loop(int cplx, int n, void *dU, void *dA, void *dZ, const int *J, double
     }
     launched += per_sync;
     g_launches += (long long)per_sync * (kStepLaunches - ((w.n_plus > 0 && w.n_minus > 0) ? 0 : 1) +
+                                         ((w.cplx && w.n_plus > 0 && w.n_minus > 0) ? 1 : 0) +
                                          (w.learned ? ((w.n_plus > 0 && w.n_minus > 0) ? 2 : 1) : 0));
     if (w.st_host->stop) { info = w.st_host->info; break; }
     if (w.st_host->steps >= cap || launched > 2 * cap + per_sync) { info = JK_ERR_MAX_STEPS; break; }

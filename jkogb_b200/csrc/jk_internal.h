@@ -82,6 +82,7 @@ struct Workspace {
   int *J;            // signs (device)
   int *plus, *minus; // indices with J=+1 / J=-1, ascending
   double *Wm;        // n x n pair weights, symmetric, NaN = no transformation
+  double *mag;       // complex: n x n magnitudes |A(i,j)| of the step
   void *hpar;        // per hyperbolic pair: scan parameters (real path), 1024 slots per 32 x 32 tile
   int *tcount;       // hyperbolic pairs per tile
   void *piv;         // Piv<T>[n/2]

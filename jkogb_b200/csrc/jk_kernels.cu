@@ -423,6 +423,133 @@ k_hyp_pm(const State *st, const double *__restrict__ A, const int *__restrict__ 
   }
 }
 
+// |A(i,j)| of every entry of a complex A (the project's hypot), once per step: the
+// column scan of ABODNZF2 needs the magnitude of every unrotated entry of its two
+// columns, and every pair of a column would otherwise compute it again
+__global__ void k_absmat(const State *st, const double2 *__restrict__ A, long long nn, double *__restrict__ mag)
+{
+  if (st->stop || st->learned_step) return;
+  for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < nn; k += (long long)gridDim.x * blockDim.x)
+    mag[k] = zabs(A[k]);
+}
+
+// ABODNZF2's row scan (src/Z/ztransf.F90:452-637) with the magnitudes of the unrotated
+// entries taken from xa, ya: the same operations in the same order as scan_rows_cplx
+__device__ __forceinline__ void scan_rows_cplx_mag(const double2 *xs, const double2 *ys, const double *xa, const double *ya,
+                                                   int rows, int i0, int p, int q, const ZRot &t, double &d)
+{
+  for (int r = 0; r < rows; ++r) {
+    double2 x = xs[r], y = ys[r];
+    zrot_apply_ab(t, x, y);
+    const int i = i0 + r;
+    if (i != p && i != q) {
+      const double axi = xa[r], axx = zabs(x), ayi = ya[r], ayy = zabs(y);
+      d = fma(__dsub_rn(axi, axx), __dadd_rn(axi, axx), d);
+      d = fma(__dsub_rn(ayi, ayy), __dadd_rn(ayi, ayy), d);
+    }
+  }
+}
+
+// The complex hyperbolic weights (ZMAGF2H, src/Z/zstep.F90:43-74): the tile of
+// k_weights_hyp with the unrotated magnitudes staged beside the columns (48 rows per
+// chunk to stay within the static shared-memory limit)
+#define ZHR 48
+template <int HP, int HM>
+__global__ void __launch_bounds__(HP * HM)
+k_weights_hyp_z(const State *st, const double2 *__restrict__ A, const double *__restrict__ mag, const int *__restrict__ plus,
+                const int *__restrict__ minus, int n_plus, int n_minus, double *__restrict__ Wm, int n)
+{
+  if (st->stop || st->learned_step) return;  // a learned step ranks these pairs by the scorer
+  __shared__ double2 sP[HP][ZHR + 1];
+  __shared__ double2 sM[HM][ZHR + 1];
+  __shared__ double aP[HP][ZHR + 1];
+  __shared__ double aM[HM][ZHR + 1];
+  const int tx = threadIdx.x % HP, ty = threadIdx.x / HP;
+  const int ia = blockIdx.x * HP + tx, ib = blockIdx.y * HM + ty;
+  const bool valid = (ia < n_plus) && (ib < n_minus);
+  int p = 0, q = 0;
+  bool scan = false, a_is_p = true;
+  double d = 0.0, w = nan_w();
+  ZRot t;
+  if (valid) {
+    const int a = plus[ia], b = minus[ib];
+    a_is_p = (a < b);
+    p = a_is_p ? a : b;
+    q = a_is_p ? b : a;
+    const double2 app = A[(long long)p * n + p], aqp = A[(long long)p * n + q], apq = A[(long long)q * n + p],
+                  aqq = A[(long long)q * n + q];
+    if (may_transform(app, aqp, apq, aqq)) {
+      double2 A2[4] = { app, aqp, apq, aqq }, U2[4], Z2[4];
+      int info = 0;
+      const int jp = a_is_p ? 1 : -1;  // "+" column a, "-" column b
+      zhsvd2(A2, jp, -jp, U2, Z2, JK_TH1FIX, info);
+      if (info < 0) w = nan_w();
+      else if (!(info & 1)) w = 0.0;
+      else if (!(info & 4)) w = dasum4(aqp.x, aqp.y, apq.x, apq.y);
+      else {
+        // the two off-diagonal terms that start ABODNZF2
+        const double2 a1 = (info & 8) ? A2[M21] : make_double2(0.0, 0.0);
+        const double2 a2 = (info & 8) ? A2[M12] : make_double2(0.0, 0.0);
+        d = 0.0;
+        d = fma(__dsub_rn(aqp.x, a1.x), __dadd_rn(aqp.x, a1.x), d);
+        d = fma(__dsub_rn(aqp.y, a1.y), __dadd_rn(aqp.y, a1.y), d);
+        d = fma(__dsub_rn(apq.x, a2.x), __dadd_rn(apq.x, a2.x), d);
+        d = fma(__dsub_rn(apq.y, a2.y), __dadd_rn(apq.y, a2.y), d);
+        t = zrot_ab(Z2);
+        scan = true;
+      }
+    }
+  }
+  if (!__syncthreads_or(scan)) {
+    if (valid) {
+      if (w < -JK_HUGE) w = nan_w();
+      Wm[(long long)q * n + p] = w;
+      Wm[(long long)p * n + q] = w;
+    }
+    return;
+  }
+  const int pa = blockIdx.x * HP, pb = blockIdx.y * HM;
+  for (int i0 = 0; i0 < n; i0 += ZHR) {
+    const int rows = min(ZHR, n - i0);
+    for (int k = threadIdx.x; k < (HP + HM) * ZHR; k += HP * HM) {
+      const int c = k / ZHR, r = k % ZHR;
+      if (r < rows) {
+        if (c < HP) {
+          const int ca = pa + c;
+          if (ca < n_plus) {
+            const long long g = (long long)plus[ca] * n + i0 + r;
+            sP[c][r] = A[g];
+            aP[c][r] = mag[g];
+          }
+        }
+        else {
+          const int cb = pb + (c - HP);
+          if (cb < n_minus) {
+            const long long g = (long long)minus[cb] * n + i0 + r;
+            sM[c - HP][r] = A[g];
+            aM[c - HP][r] = mag[g];
+          }
+        }
+      }
+    }
+    __syncthreads();
+    if (scan) {
+      const double2 *xs = a_is_p ? sP[tx] : sM[ty];
+      const double2 *ys = a_is_p ? sM[ty] : sP[tx];
+      const double *xa = a_is_p ? aP[tx] : aM[ty];
+      const double *ya = a_is_p ? aM[ty] : aP[tx];
+      scan_rows_cplx_mag(xs, ys, xa, ya, rows, i0, p, q, t, d);
+    }
+    __syncthreads();
+  }
+  if (valid) {
+    if (scan) w = d;
+    if (w < -JK_HUGE) w = nan_w();
+    Wm[(long long)q * n + p] = w;
+    Wm[(long long)p * n + q] = w;
+  }
+}
+
 template <typename T, int HP, int HM>
 __global__ void __launch_bounds__(HP * HM)
 k_weights_hyp(const State *st, const T *__restrict__ A, const int *__restrict__ plus, const int *__restrict__ minus,
@@ -1296,6 +1423,22 @@ static cudaError_t weights_t(Workspace &w, const T *A, cudaStream_t s)
     // the pipelined real kernel once its tiles fill the GPU; 16 x 16 / 8 x 8 tiles otherwise
     if (sizeof(T) == sizeof(double) && (long long)w.n_plus * w.n_minus >= 512LL * 148 * 2) {
       hyp_d_launch(w, (const double *)A, s);
+    }
+    else if (sizeof(T) == sizeof(double2)) {
+      // complex: the magnitudes of all entries once, then the tiles
+      const long long nn = (long long)n * n;
+      k_absmat<<<(unsigned)((nn + 255) / 256 < 4096 ? (nn + 255) / 256 : 4096), 256, 0, s>>>(w.st, (const double2 *)A, nn,
+                                                                                              w.mag);
+      if ((long long)w.n_plus * w.n_minus >= 256LL * 148 * 4) {
+        dim3 gh((w.n_plus + 15) / 16, (w.n_minus + 15) / 16);
+        k_weights_hyp_z<16, 16><<<gh, 256, 0, s>>>(w.st, (const double2 *)A, w.mag, w.plus, w.minus, w.n_plus, w.n_minus,
+                                                  w.Wm, n);
+      }
+      else {
+        dim3 gh((w.n_plus + 7) / 8, (w.n_minus + 7) / 8);
+        k_weights_hyp_z<8, 8><<<gh, 64, 0, s>>>(w.st, (const double2 *)A, w.mag, w.plus, w.minus, w.n_plus, w.n_minus,
+                                               w.Wm, n);
+      }
     }
     else if ((long long)w.n_plus * w.n_minus >= 256LL * 148 * 4) {
       dim3 gh((w.n_plus + 15) / 16, (w.n_minus + 15) / 16);
