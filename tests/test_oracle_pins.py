@@ -100,3 +100,49 @@ def test_thread_count_determinism():
     assert np.array_equal(a["trace"]["piv"], b["trace"]["piv"])
     for k in ("U", "Z", "sigma"):
         assert np.array_equal(a[k], b[k])
+
+
+def test_pair_order_and_ncp_strategies_equivalent():
+    # TRU1 and TRU2 list the pairs differently, but the record sort is a total order, so the
+    # loop's results do not depend on it; NCP1 and NCP2 take the same greedy set
+    import numpy as np
+    import oracle
+    from jkogb_b200 import gen
+    Y, J = gen.graded(20, 1e-3, seed=12)
+    base = oracle.step_loop(Y, J, id_ncp=2, id_tru=1, nt=1, trace=True)
+    for ncp, tru, nt in ((1, 1, 3), (2, 2, 1), (1, 2, 2)):
+        r = oracle.step_loop(Y, J, id_ncp=ncp, id_tru=tru, nt=nt, trace=True)
+        assert r["info"] == base["info"]
+        assert np.array_equal(r["trace"]["piv"], base["trace"]["piv"])
+        for k in ("A", "U", "Z", "sigma"):
+            assert np.array_equal(np.ascontiguousarray(r[k]).view(np.uint8), np.ascontiguousarray(base[k]).view(np.uint8))
+
+
+def test_ncp3_takes_the_best_walk():
+    # AW_NCP3's pick is the walk of largest value among all start offsets; it is one of
+    # the walks, and its value is at least the plain walk's (start offset 1)
+    import numpy as np
+    import oracle
+    from jkogb_b200 import gen
+    Y, J = gen.graded(14, 1e-2, seed=13)
+    w, P, Q, _ = oracle.weights(Y, J)
+    p2 = oracle.select(14, w, P, Q, 7, id_ncp=2)
+    p3 = oracle.select(14, w, P, Q, 7, id_ncp=3)
+    W = {(int(a), int(b)): x for a, b, x in zip(P, Q, w)}
+
+    def value(piv):
+        ws = [W[(int(a), int(b))] for a, b in piv]
+        last = max([k for k, x in enumerate(ws) if x > 0], default=-1)
+        wp = 0.0
+        for k in range(last, -1, -1):
+            wp += ws[k]
+        wn = 0.0
+        for k in range(last + 1, len(ws)):
+            wn += ws[k]
+        return wp + wn
+
+    assert value(p3) >= value(p2)
+    used = set()
+    for a, b in p3:
+        assert a not in used and b not in used
+        used |= {int(a), int(b)}
