@@ -69,8 +69,12 @@ def rank_batch_seed(rank):
 
 
 def _clock_sampler(dev):
-    f = open(os.path.join(ROOT, "gpurun_out" if os.path.isdir(os.path.join(ROOT, "gpurun_out")) else ".",
-                          f".clocks_{os.getpid()}.csv"), "w")
+    """nvidia-smi sampling the GPU's clocks and throttle reasons every 200 ms into a
+    temporary file, for the duration of the timed region."""
+    import tempfile
+    fd, name = tempfile.mkstemp(prefix="jk_clocks_", suffix=".csv")
+    os.close(fd)
+    f = open(name, "w")
     q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
          "clocks_event_reasons.sw_power_cap")
@@ -84,6 +88,8 @@ def _clock_sampler(dev):
 
 def _clock_summary(p, f):
     if p is None:
+        f.close()
+        os.unlink(f.name)
         return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
     p.terminate()
     try:

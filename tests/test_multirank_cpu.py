@@ -46,3 +46,24 @@ def test_two_gloo_ranks_time_and_partition():
 def test_single_process_max_is_identity():
     import bench
     assert bench.max_over_ranks(3.5) == 3.5
+
+
+def test_clock_summary_parses_samples():
+    import bench
+
+    class _Done:
+        def terminate(self):
+            pass
+
+        def wait(self, t):
+            pass
+
+    p, f = bench._clock_sampler(0)
+    if p is not None:
+        p.terminate()
+        p.wait()
+    f.write("0, 1965, 1965, 500.0, 0x0, Not Active, Not Active, Not Active, Active\n")
+    f.write("0, 1900, 1965, 900.0, 0x4, Not Active, Active, Not Active, Not Active\n")
+    c = bench._clock_summary(_Done(), f)
+    assert c["sm_mhz"] == 1932.5 and c["sm_max_mhz"] == 1965.0
+    assert c["reasons"] == ["hw_thermal_slowdown", "sw_power_cap"]
