@@ -58,10 +58,10 @@ def test_clock_summary_parses_samples():
         def wait(self, t):
             pass
 
-    p, f = bench._clock_sampler(0)
-    if p is not None:
-        p.terminate()
-        p.wait()
+    import tempfile
+    fd, name = tempfile.mkstemp(suffix=".csv")
+    os.close(fd)
+    f = open(name, "w")
     f.write("0, 1965, 1965, 500.0, 0x0, Not Active, Not Active, Not Active, Active\n")
     f.write("0, 1900, 1965, 900.0, 0x4, Not Active, Active, Not Active, Not Active\n")
     c = bench._clock_summary(_Done(), f)
