@@ -1,12 +1,13 @@
 """Benchmark of the J-Kogbetliantz HSVD step loop on B200 (time to converge, solves/s).
 
-One benchmark step is one full solve (DSTEP_LOOP from Y to U, Z, SIGMA) of the
-workload: the real N = 2048 graded matrix Y = G D (G iid N(0,1), D log-uniform in
-[1e-6, 1], seeded), J with 1024 entries of each sign in a seeded permutation,
-N_2 = 1024.  `value` times the solve on device-resident inputs; `e2e` times the
-same solve through the host-pointer C ABI (the call a user makes), host copies
-included.  Multi-GPU runs (torchrun, one process per GPU) solve one replica per
-rank (weak scaling, no collective on the data path).
+The workload is one full solve (DSTEP_LOOP from Y to U, Z, SIGMA) of the real
+N = 2048 graded matrix Y = G D (G iid N(0,1), D log-uniform in [1e-6, 1], seeded),
+J with 1024 entries of each sign in a seeded permutation, N_2 = 1024.  The timed
+region is that one solve on device-resident inputs, cut at solver-step boundaries
+into --steps slices (one benchmark step = one slice); `value` is solves/s.  `e2e`
+times one solve through the host-pointer C ABI (the call a user makes), host
+allocation and copies included.  Multi-GPU runs (torchrun, one process per GPU)
+solve one replica per rank (weak scaling, no collective on the data path).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
 """
@@ -38,9 +39,10 @@ WORKLOADS = {
                      desc="Y iid N(0,1), seed 1; J = 192 x +1 then 64 x -1; N_2 = 128"),
     "zjk_n1024": dict(kind="complex", n=1024, n_2=512, make=lambda: gen.complex_gaussian(1024, seed=3),
                       desc="Y complex, Re/Im iid N(0,1/2), seed 3; J = 512 x +1 then 512 x -1; N_2 = 512"),
-    "batch4096": dict(kind="batch", count=4096, make=lambda seed=4: gen.batch(4096, 16, 128, seed=seed),
+    "batch4096": dict(kind="batch", count=4096, make=lambda: gen.batch(4096, 16, 128, seed=4),
                       desc="4096 real matrices, even N uniform in [16,128], Y iid N(0,1), J iid +-1 with "
-                           "P(+1) ~ U[0.2,0.8] per matrix, N_2 = N/2; seed 4 (+ rank); one persistent launch"),
+                           "P(+1) ~ U[0.2,0.8] per matrix, N_2 = N/2; seed 4; one persistent launch per rank "
+                           "over the rank's share of the batch"),
 }
 STEPS_FILE = os.path.join(ROOT, "bench_steps.json")
 
@@ -61,11 +63,6 @@ def max_over_ranks(x, device=None):
     if dist.is_available() and dist.is_initialized() and dist.get_world_size() > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
-
-
-def rank_batch_seed(rank):
-    """The batched workload's seed on a rank: every rank solves its own 4096-matrix batch."""
-    return 4 + int(rank)
 
 
 def _clock_sampler(dev):
@@ -175,32 +172,39 @@ _batch_js = []
 
 
 def run_reference(args, wl):
+    """The oracle port (the reference's algorithm, restated in C with OpenMP) on all host
+    cores: --warmup solver steps, then exactly --steps solver steps timed, both from the
+    start of the solve; the time to converge is extrapolated with the recorded step count."""
     ws, rank, _ = _dist()
     if rank != 0:
         return
     if wl["kind"] == "batch":
         return run_reference_batch(args, wl)
+    import oracle
     Y, J = wl["make"]()
     rec = _steps_record().get(args.workload)
     if not rec:
         print(json.dumps({"impl": "reference", "unavailable": "no recorded step count for this workload"}))
         return
-    for _ in range(args.warmup):
-        cpu_sample(Y, J, wl["n_2"], max_seconds=5.0)
-    per = []
-    for _ in range(args.steps):
-        sec, nsteps, nt = cpu_sample(Y, J, wl["n_2"], max_seconds=20.0)
-        per.append(sec)
-    sec = float(np.mean(per))
+    nt = os.cpu_count() or 1
+    if args.warmup > 0:
+        oracle.step_loop(Y, J, n_2=wl["n_2"], nt=nt, stop_after=args.warmup)
+    t0 = time.perf_counter()
+    oracle.step_loop(Y, J, n_2=wl["n_2"], nt=nt, stop_after=args.steps)
+    dt = time.perf_counter() - t0
+    sec = dt / args.steps
     solve_s = sec * rec
     out = {
         "impl": "reference", "metric": "HSVD time-to-converge & solves/s", "value": 1.0 / solve_s, "unit": "solves/s",
-        "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": solve_s * 1e3,
+        "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": args.workload, "desc": wl["desc"], "steps_to_converge": rec},
+        "config": {"workload": args.workload, "desc": wl["desc"],
+                   "step": "one benchmark step = one solver step (DSTEP_BUILD + DSTEP_TRANSF) from the start of the solve",
+                   "solver_steps_to_converge": rec, "ms_per_solver_step": sec * 1e3,
+                   "extrapolated_solve_s": solve_s},
         "cpu_baseline": {"value": 1.0 / solve_s, "unit": "solves/s", "cores": nt, "kind": "port",
-                         "sample": f"{nsteps} solver steps from the start of the solve, timed per step and "
-                                   f"multiplied by the {rec} steps the solve takes"},
+                         "sample": f"{args.steps} solver steps from the start of the solve ({sec:.3f} s/step), "
+                                   f"extrapolated to the {rec} steps the solve takes"},
         "e2e": {"value": 1.0 / solve_s, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(out))
@@ -233,10 +237,15 @@ def run_reference_batch(args, wl):
 
 
 def run_ours_batch(args, wl):
+    """One 4096-matrix batch, partitioned over the ranks by estimated cost (N^4, the
+    longest-processing-time rule); each rank solves its share in one persistent launch per
+    benchmark step; rank 0 gathers every matrix's INFO.  `value` counts the matrices that
+    converged (INFO >= 0) per second of the slowest rank."""
     import torch
     import torch.distributed as dist
 
     import jkogb_b200 as jk
+    from jkogb_b200 import partition
 
     ws, rank, local = _dist()
     if ws > 1:
@@ -245,9 +254,11 @@ def run_ours_batch(args, wl):
         dist.init_process_group("nccl", timeout=timedelta(seconds=900), device_id=torch.device("cuda", local))
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
-    b = wl["make"](seed=rank_batch_seed(rank))  # one batch per rank: no collective on the data path
-    mats = [Y for Y, _ in b]
-    Js = [J for _, J in b]
+    b = wl["make"]()
+    total = len(b)
+    share = partition.partition([Y.shape[0] for Y, _ in b], ws)[rank]
+    mats = [b[i][0] for i in share]
+    Js = [b[i][1] for i in share]
     A, J, n, off = jk.batch_pack(mats, Js)
     cnt = len(n)
     plan = jk.Batch(n, np.zeros(cnt, np.int32), J)
@@ -286,7 +297,7 @@ def run_ours_batch(args, wl):
         launches += 1
     barrier()
     clocks = _clock_summary(smi, smf)
-    dev_ms = sum(a.elapsed_time(b) for a, b in ev)
+    dev_ms = sum(a.elapsed_time(b_) for a, b_ in ev)
     ms = max_over_ranks(dev_ms, dev) / args.steps
     info = di.cpu().numpy()
     plan.close()
@@ -294,34 +305,37 @@ def run_ours_batch(args, wl):
     # end to end: the host-pointer entry (copies in and out inside the call)
     barrier()
     tt0 = time.perf_counter()
-    for _ in range(args.steps):
-        res = jk.dstep_loop_batched(mats, Js)
-    e2e_s = (time.perf_counter() - tt0) / args.steps
-    e2e_s = max_over_ranks(e2e_s, dev)
+    res = jk.dstep_loop_batched(mats, Js)
+    e2e_s = max_over_ranks(time.perf_counter() - tt0, dev)
     same = bool(np.array_equal(np.array([r["info"] for r in res]), info))
 
-    # FP64 work of the weight scans of the whole batch: sum over matrices and steps of
+    # FP64 work of the weight scans of this rank's share: sum over matrices and steps of
     # NH (N - 2) 14 flop, with each matrix's NH and step count
     nplus = np.array([int(np.sum(j == 1)) for j in Js])
     steps_pos = np.where(info > 0, info, 0).astype(np.float64)
     flops = float(np.sum(steps_pos * nplus * (n - nplus) * (n - 2) * 14.0))
     achieved = flops / (ms * 1e-3) / 1e12
     peak = jk.lib().jk_fp64_peak()
+    infos = partition.gather_results(share, [int(x) for x in info], total) if ws > 1 else [int(x) for x in info]
     if ws > 1:
         dist.barrier()
         dist.destroy_process_group()
     if rank != 0:
         return
+    infos = np.array(infos)
+    conv = int(np.sum(infos >= 0))
     out = {
-        "metric": "HSVD time-to-converge & solves/s", "value": ws * cnt * 1e3 / ms, "unit": "solves/s",
+        "metric": "HSVD time-to-converge & solves/s", "value": conv * 1e3 / ms, "unit": "solves/s",
         "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded generator, the workload's distributions)",
-        "config": {"workload": args.workload, "desc": wl["desc"], "matrices": cnt, "threads_per_block": threads,
-                   "parallelism": f"partition{ws}", "steps_total": int(steps_pos.sum()),
-                   "matrices_over_100N_steps": int(np.sum(info > 100 * n)), "matrices_step_capped": int(np.sum(info == -24)),
+        "config": {"workload": args.workload, "desc": wl["desc"], "matrices": total, "matrices_converged": conv,
+                   "matrices_step_capped": int(np.sum(infos == -24)), "threads_per_block": threads,
+                   "parallelism": f"partition{ws} (longest-processing-time on N^4)",
+                   "steps_total_rank0": int(steps_pos.sum()),
+                   "matrices_over_100N_steps_rank0": int(np.sum(info > 100 * n)),
                    "l2": "each block's matrix lives in shared memory; U, Z (<= 0.5 GB) stream through L2"},
-        "e2e": {"value": ws * cnt / e2e_s, "unit": "solves/s", "h2d_bytes_per_step": int(A.nbytes + J.nbytes),
+        "e2e": {"value": conv / e2e_s, "unit": "solves/s", "h2d_bytes_per_step": int(A.nbytes + J.nbytes),
                 "d2h_bytes_per_step": int(3 * A.nbytes + 8 * int(n.sum()) + 4 * cnt), "same_info": same},
         "gpu_launches": launches,
         "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
@@ -340,6 +354,10 @@ def run_ours_batch(args, wl):
 
 
 def run_ours(args, wl):
+    """One full device-resident solve, cut into --steps slices of solver steps (the
+    recorded step count / K each, the last slice to the end), each slice timed with CUDA
+    events on the solver's stream; --warmup bounded prefix solves (32 steps each) before
+    it; then one end-to-end solve through the host-pointer C ABI."""
     import torch
     import torch.distributed as dist
 
@@ -362,53 +380,61 @@ def run_ours(args, wl):
     Z = torch.empty((n, n), dtype=tdt, device=dev).t()
     s = torch.empty(n, dtype=torch.float64, device=dev)
     stream = torch.cuda.current_stream(dev)
-
-    def device_solve():
-        A.copy_(Y0)
-        return jk.step_loop_dev(A, U, Z, s, J, n_2=n_2, stream=stream)
+    sp = stream.cuda_stream
+    solver = jk.Solver(n, J, n_2=n_2, complex_=cplx)
+    ptrs = (U.data_ptr(), A.data_ptr(), Z.data_ptr())
 
     def barrier():
         if ws > 1:
             dist.barrier()
         torch.cuda.synchronize(dev)
 
-    info = None
+    # warm-up: bounded prefixes of the same solve (graph capture, first launches)
     for _ in range(args.warmup):
-        info = device_solve()
+        A.copy_(Y0)
+        solver.begin(*ptrs, sp)
+        solver.advance(32)
+        solver.finish(s.data_ptr())
+    rec = _steps_record().get(args.workload) or 32 * args.steps
+    per_slice = -(-int(rec) // args.steps)
+    A.copy_(Y0)  # the input, restored outside the timed region
     barrier()
     smi, smf = _clock_sampler(local)
-    launches = 0
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.steps):
-        info = device_solve()
-        launches += jk.lib().jk_last_launch_count()
-    e1.record(stream)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    ev[0].record(stream)
+    solver.begin(*ptrs, sp)
+    for k in range(args.steps):
+        solver.advance(per_slice if k < args.steps - 1 else 0)
+        if k == args.steps - 1:
+            info = solver.finish(s.data_ptr())
+        ev[k + 1].record(stream)
+    launches = int(jk.lib().jk_last_launch_count())  # the solve's launches, begin to finish
     barrier()
     clocks = _clock_summary(smi, smf)
-    dev_ms = e0.elapsed_time(e1)
-    ms_per_solve = max_over_ranks(dev_ms, dev) / args.steps
+    slice_ms = [ev[k].elapsed_time(ev[k + 1]) for k in range(args.steps)]
+    dev_ms = sum(slice_ms)
+    solve_ms = max_over_ranks(dev_ms, dev)
+    sig_dev = s.cpu().numpy()
+    solver.close()
 
-    # end to end: the host-pointer C ABI (H2D of Y, D2H of U, Z, SIGMA inside the call)
+    # end to end: one solve through the host-pointer C ABI (H2D of Y, D2H of A, U, Z, SIGMA inside)
     Yh = np.asfortranarray(Y)
     barrier()
     tt0 = time.perf_counter()
-    for _ in range(args.steps):
-        r = jk.step_loop(Yh, J, n_2=n_2)
-    e2e_s = (time.perf_counter() - tt0) / args.steps
-    e2e_s = max_over_ranks(e2e_s, dev)
-    ok = bool(r["info"] == info)
+    r = jk.step_loop(Yh, J, n_2=n_2)
+    e2e_s = max_over_ranks(time.perf_counter() - tt0, dev)
+    same = bool(r["info"] == info and np.array_equal(r["sigma"].view(np.uint64), sig_dev.view(np.uint64)))
 
     # the dominant kernel (the pair weights) timed alone on the workload's input
     h = jk.Handle(n, J, complex_=cplx)
     for _ in range(3):
-        h.weights(Y0.data_ptr(), None, stream.cuda_stream)
+        h.weights(Y0.data_ptr(), None, sp)
     torch.cuda.synchronize(dev)
     w0, w1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     reps = 10
     w0.record(stream)
     for _ in range(reps):
-        h.weights(Y0.data_ptr(), None, stream.cuda_stream)
+        h.weights(Y0.data_ptr(), None, sp)
     w1.record(stream)
     torch.cuda.synchronize(dev)
     w_ms = w0.elapsed_time(w1) / reps
@@ -429,14 +455,20 @@ def run_ours(args, wl):
     h2d = n * n * esize + n * 4
     d2h = 3 * n * n * esize + n * 8
     out = {
-        "metric": "HSVD time-to-converge & solves/s", "value": ws * 1e3 / ms_per_solve, "unit": "solves/s",
-        "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_solve,
+        "metric": "HSVD time-to-converge & solves/s", "value": ws * 1e3 / solve_ms, "unit": "solves/s",
+        "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": solve_ms / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128" if cplx else "f64",
         "data": "synthetic (seeded generator, the workload's distributions)",
-        "config": {"workload": args.workload, "desc": wl["desc"], "n": n, "n_2": n_2, "steps_to_converge": info,
+        "config": {"workload": args.workload, "desc": wl["desc"], "n": n, "n_2": n_2,
+                   "step": "one benchmark step = 1/K of one full solve (the solve cut at solver-step "
+                           f"boundaries into K = {args.steps} slices of {per_slice} solver steps, the last to the end)",
+                   "solver_steps_to_converge": info, "ms_per_solver_step": solve_ms / max(info, 1),
+                   "slice_ms": [round(x, 3) for x in slice_ms],
+                   "warmup": f"{args.warmup} prefix solves of 32 solver steps",
                    "parallelism": f"replicas{ws}", "l2": "working set > L2 (A, U, Z, W: 4 x 32 MB + ranking lists)"},
         "e2e": {"value": ws / e2e_s, "unit": "solves/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                "same_info": ok},
+                "what": "one solve through jk_dstep_loop (host buffers, allocation and copies inside)",
+                "same_result_as_device_solve": same},
         "gpu_launches": launches,
         "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                      "frac": achieved / peak if peak > 0 else None, "traffic": traffic,
@@ -451,7 +483,7 @@ def run_ours(args, wl):
         steps_conv = info if info and info > 0 else _steps_record().get(args.workload)
         out["cpu_baseline"] = {"value": 1.0 / (sec * steps_conv), "unit": "solves/s", "cores": nt, "kind": "port",
                                "sample": f"{nsteps} solver steps of the same solve on all host cores "
-                                         f"({sec:.3f} s/step) x {steps_conv} steps to converge"}
+                                         f"({sec:.3f} s/step) x {steps_conv} steps to converge (extrapolated)"}
     print(json.dumps(out))
 
 

@@ -4,7 +4,7 @@
  *
  * The entry points replace the Fortran seam the reference's drivers call:
  *   DSTEP_LOOP(N, U, LDU, A, LDA, Z, LDZ, J, SIGMA, NN, P, Q, R, NM, DZ, N_2, STEP, TT, W, INFO)
- *     src/D/dstep.F90:472-604, called from src/D/djk.F90:253
+ *     src/D/dstep.F90:472-604, called from src/D/djk.F90:83
  *   ZSTEP_LOOP(...)  src/Z/zstep.F90:482-615, called from src/Z/zjk.F90
  * together with the strategy plug-ins DPROC_INIT selects (src/D/dstep.F90:76-134):
  * ID_NCP 0/1/2 (greedy non-colliding selection, AW_NCP1 == AW_NCP2), 3 (AW_NCP3, the best
@@ -31,7 +31,8 @@ extern "C" {
 
 /* Options; a NULL pointer means all defaults (zero). */
 typedef struct {
-  int max_steps;    /* stop after this many steps (0: no limit); INFO = JK_ERR_MAX_STEPS when hit */
+  int max_steps;    /* stop after this many steps (0: no limit, as DSTEP_LOOP, src/D/dstep.F90:564-578);
+                       INFO = JK_ERR_MAX_STEPS when hit, with A, U, Z, SIGMA as the loop left them */
   int zba_quirk;    /* complex BA branch of src/Z/ztransf.F90:325: 0 = as the reference (R1), 1 = R2 as the real code */
   int graph_steps;  /* steps per CUDA-graph launch (0: 32; -1: plain stream launches) */
   int device;       /* CUDA device ordinal for the host-pointer entry points (-1 or 0: current) */
@@ -61,6 +62,8 @@ typedef struct {
 #define JK_ERR_MAX_STEPS (-24)  /* opts->max_steps reached */
 #define JK_ERR_NO_DEVICE (-33)  /* no CUDA device */
 #define JK_ERR_SCRATCH (-34)    /* N beyond JK_NOALLOC_MAX_N (jk_dweights_noalloc) */
+#define JK_ERR_STALL (-26)      /* internal: the device loop neither advanced nor ended (a library fault) */
+#define JK_ERR_STATE (-27)      /* a jk_solver call out of order (advance or finish before begin) */
 
 /* DSTEP_LOOP with host buffers, src/D/dstep.F90:472-604 (copies to and from the device).
  * A is in/out; U, Z, SIGMA are out.  N_2 is clamped as JSTEP_LEN does (src/shared/jstep.F90:124). */
@@ -78,6 +81,38 @@ int jk_dstep_loop_dev(int n, double *dU, double *dA, double *dZ, const int *J, d
                       int n_2, int id_ncp, int id_tru, const jk_opts *opts, jk_trace *trace, void *stream);
 int jk_zstep_loop_dev(int n, double *dU, double *dA, double *dZ, const int *J, double *dsigma,
                       int n_2, int id_ncp, int id_tru, const jk_opts *opts, jk_trace *trace, void *stream);
+
+/* The same loop as a reusable object that can be advanced a given number of steps at a
+ * time: the caller-owned workspace of DSTEP_LOOP (DZ, STEP, W, P, Q: src/D/djk.F90:47-56)
+ * made once per order N, sign vector J, N_2 and strategy, and the loop of
+ * src/D/dstep.F90:564-583 split at step boundaries.  Results are those of
+ * jk_dstep_loop_dev / jk_zstep_loop_dev, whatever the split.
+ *   create   the device workspace (J a host array; opts: max_steps, zba_quirk,
+ *            graph_steps, device); NULL on error with *info set
+ *   begin    a new solve on device buffers (leading dimension n, complex: interleaved):
+ *            A in/out, U and Z out; enqueues U = Z = I and the loop-state reset on `stream`
+ *   resume   a solve that an earlier loop left unfinished after `steps` steps (INFO
+ *            JK_ERR_MAX_STEPS): A, U, Z as that loop returned them (diagonal in SIGMA,
+ *            Z already J Z^T J); restores the loop's state from them and continues, so
+ *            that the final results equal one uninterrupted solve's
+ *   advance  runs the loop until S has grown by `steps` (0: until the loop ends) and
+ *            returns 1 when the loop has ended, 0 when it stopped at that count, < 0 on
+ *            error; synchronises the stream once per graph launch (32 steps by default)
+ *   steps    S so far (steps with effective transformations)
+ *   finish   SIGMA := diag(A), A's diagonal zeroed, Z := J Z^T J (J Z^H J); returns
+ *            INFO as DSTEP_LOOP: S when the loop ended, JK_ERR_MAX_STEPS when it stopped
+ *            at opts->max_steps or was not advanced to its end, < 0 on an error
+ * A solver is used by one host thread at a time. */
+typedef struct jk_solver jk_solver;
+jk_solver *jk_solver_create(int n, int complex_, const int *J, int n_2, int id_ncp, int id_tru, const jk_opts *opts,
+                            int *info);
+void jk_solver_destroy(jk_solver *s);
+int jk_solver_begin(jk_solver *s, double *dU, double *dA, double *dZ, void *stream);
+int jk_solver_resume(jk_solver *s, double *dU, double *dA, double *dZ, const double *dsigma, long long steps,
+                     void *stream);
+int jk_solver_advance(jk_solver *s, long long steps);
+long long jk_solver_steps(const jk_solver *s);
+int jk_solver_finish(jk_solver *s, double *dsigma);
 
 /* A batch of independent 2x2 HSVDs on the device (DHSVD2 src/D/dtransf.F90:614,
  * ZHSVD2 src/Z/ztransf.F90:925; the dtest/ztest kernel).  Host arrays: A, U, Z hold

@@ -23,13 +23,15 @@ import numpy as np
 
 __all__ = ["lib", "step_loop", "dstep_loop", "zstep_loop", "step_loop_dev", "hsvd2_batch", "weights", "select",
            "read_yj", "write_uzs", "JkError", "jstep_len", "SYMBOLS", "weights_noalloc",
-           "NOALLOC_MAX_N", "dstep_loop_batched", "Batch", "batch_pack", "batch_unpack", "BATCH_MAX_N"]
+           "NOALLOC_MAX_N", "dstep_loop_batched", "Batch", "batch_pack", "batch_unpack", "BATCH_MAX_N", "Solver"]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "_lib", "libjkogb_b200.so")
 
 # every symbol include/jkogb.h declares
-SYMBOLS = ("jk_dstep_loop", "jk_zstep_loop", "jk_dstep_loop_dev", "jk_zstep_loop_dev", "jk_dhsvd2_batch",
+SYMBOLS = ("jk_dstep_loop", "jk_zstep_loop", "jk_dstep_loop_dev", "jk_zstep_loop_dev", "jk_solver_create",
+           "jk_solver_destroy", "jk_solver_begin", "jk_solver_resume", "jk_solver_advance", "jk_solver_steps",
+           "jk_solver_finish", "jk_dhsvd2_batch",
            "jk_zhsvd2_batch", "jk_dweights", "jk_zweights", "jk_select", "jk_handle_create", "jk_handle_destroy",
            "jk_handle_weights", "jk_dweights_noalloc", "jk_batch_create", "jk_batch_destroy",
            "jk_batch_run", "jk_batch_tune", "jk_dstep_loop_batched", "jk_mlp_nparams", "jk_scorer_create",
@@ -77,6 +79,20 @@ def lib():
             f = getattr(L, nm)
             f.restype = C.c_int
             f.argtypes = [C.c_int, vp, vp, vp, ip, vp, C.c_int, C.c_int, C.c_int, C.POINTER(Opts), C.POINTER(Trace), vp]
+        L.jk_solver_create.restype = C.c_void_p
+        L.jk_solver_create.argtypes = [C.c_int, C.c_int, ip, C.c_int, C.c_int, C.c_int, C.POINTER(Opts), ip]
+        L.jk_solver_destroy.restype = None
+        L.jk_solver_destroy.argtypes = [C.c_void_p]
+        L.jk_solver_begin.restype = C.c_int
+        L.jk_solver_begin.argtypes = [C.c_void_p, vp, vp, vp, vp]
+        L.jk_solver_resume.restype = C.c_int
+        L.jk_solver_resume.argtypes = [C.c_void_p, vp, vp, vp, vp, C.c_longlong, vp]
+        L.jk_solver_advance.restype = C.c_int
+        L.jk_solver_advance.argtypes = [C.c_void_p, C.c_longlong]
+        L.jk_solver_steps.restype = C.c_longlong
+        L.jk_solver_steps.argtypes = [C.c_void_p]
+        L.jk_solver_finish.restype = C.c_int
+        L.jk_solver_finish.argtypes = [C.c_void_p, vp]
         for nm in ("jk_dhsvd2_batch", "jk_zhsvd2_batch"):
             f = getattr(L, nm)
             f.restype = C.c_int
@@ -229,6 +245,65 @@ def step_loop_dev(A, U, Z, sigma, J, n_2=0, id_ncp=0, id_tru=0, stream=None, max
     if info < 0 and info != -24:
         raise JkError(info, "device step loop: ")
     return info
+
+
+class Solver:
+    """The step loop as a reusable object (jk_solver_*): one workspace for an order n, sign
+    vector J, N_2 and strategy, advanced a given number of steps at a time on device
+    buffers.  Pointers are raw device addresses (e.g. tensor.data_ptr()) of column-major
+    n x n buffers; `stream` is a raw cudaStream_t."""
+
+    def __init__(self, n, J, n_2=0, complex_=False, id_ncp=0, id_tru=0, max_steps=0, zba_quirk=0, graph_steps=0):
+        Jc = np.ascontiguousarray(np.asarray(J).astype(np.int32))
+        info = C.c_int(0)
+        self.n = int(n)
+        o = _opts(max_steps, zba_quirk, graph_steps)
+        self._s = lib().jk_solver_create(self.n, int(bool(complex_)), Jc.ctypes.data_as(C.POINTER(C.c_int)), int(n_2),
+                                          int(id_ncp), int(id_tru), C.byref(o), C.byref(info))
+        if not self._s:
+            raise JkError(info.value, "solver: ")
+
+    def begin(self, dU, dA, dZ, stream=0):
+        """Start a solve: A (in/out) is the input matrix, U = Z = I."""
+        rc = lib().jk_solver_begin(self._s, C.c_void_p(dU), C.c_void_p(dA), C.c_void_p(dZ), C.c_void_p(stream))
+        if rc < 0:
+            raise JkError(rc, "solver begin: ")
+
+    def resume(self, dU, dA, dZ, dsigma, steps, stream=0):
+        """Continue a real loop that stopped after `steps` steps (A, U, Z, SIGMA as it left them)."""
+        rc = lib().jk_solver_resume(self._s, C.c_void_p(dU), C.c_void_p(dA), C.c_void_p(dZ), C.c_void_p(dsigma),
+                                    int(steps), C.c_void_p(stream))
+        if rc < 0:
+            raise JkError(rc, "solver resume: ")
+
+    def advance(self, steps=0):
+        """Run until S has grown by `steps` (0: to the end); True once the loop has ended."""
+        rc = lib().jk_solver_advance(self._s, int(steps))
+        if rc < 0:
+            raise JkError(rc, "solver advance: ")
+        return rc == 1
+
+    @property
+    def steps(self):
+        return int(lib().jk_solver_steps(self._s))
+
+    def finish(self, dsigma):
+        """SIGMA, the zeroed diagonal, J Z^T J; returns INFO (JK_ERR_MAX_STEPS if not ended)."""
+        info = lib().jk_solver_finish(self._s, C.c_void_p(dsigma))
+        if info < 0 and info != -24:
+            raise JkError(info, "solver finish: ")
+        return info
+
+    def close(self):
+        if self._s:
+            lib().jk_solver_destroy(self._s)
+            self._s = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def hsvd2_batch(B, J, th1=0.75):

@@ -99,11 +99,6 @@ int make_workspace(Guard &g, Workspace &w, int n, int cplx, const int *J, int tr
   CK(g.alloc(&w.minus, (minus.size() + 1) * sizeof(int)));
   CK(g.alloc(&w.Wm, (size_t)n * n * sizeof(double)));
   if (cplx) CK(g.alloc(&w.mag, (size_t)n * n * sizeof(double)));
-  {
-    const size_t T = (n + 31) / 32, nt = T * (T + 1) / 2;
-    CK(g.alloc(&w.hpar, nt * 1024 * sizeof(HypPar)));
-    CK(g.alloc(&w.tcount, nt * sizeof(int)));
-  }
   CK(g.alloc(&w.piv, half * pivsz));
   CK(g.alloc(&w.rowrot, half * rrsz));
   CK(g.alloc(&w.list, (size_t)n * ((n + 7) & ~7) * sizeof(unsigned short)));
@@ -148,23 +143,47 @@ struct jk_scorer {
   int stall_k = 8;
 };
 
-namespace {
-
-// the loop of DSTEP_LOOP / ZSTEP_LOOP on device buffers
-int run_loop(int cplx, int n, void *dU, void *dA, void *dZ, const int *J, double *dsigma, int n_2, int id_ncp, int id_tru,
-             const jk_opts *opts, jk_trace *trace, cudaStream_t s, const jk_scorer *sc = nullptr, int *exact_steps = nullptr)
-{
-  (void)id_tru;  // the pair order does not change the sorted records
-  jk_opts o;
-  memset(&o, 0, sizeof(o));
-  if (opts) o = *opts;
-  n_2 = jstep_len(n, n_2);
+// The step loop of DSTEP_LOOP / ZSTEP_LOOP (src/D/dstep.F90:564-583, src/Z/zstep.F90:575-594)
+// on device buffers, resumable between steps: the workspace, the graph of `chunk`
+// whole steps and the loop's position.
+struct jk_solver {
   Guard g;
   Workspace w;
-  const int trace_on = (trace != nullptr);
-  int rc = make_workspace(g, w, n, cplx, J, trace_on, trace ? trace->max_steps : 0, trace ? trace->max_piv : 0);
+  jk_opts o;
+  int n = 0, cplx = 0, n_2 = 0;
+  int chunk = 32;                  // steps per graph launch; -1: plain stream launches
+  cudaGraphExec_t exec = nullptr;  // the captured steps, for the buffers in `key`
+  const void *key[4] = {};
+  void *dA = nullptr, *dU = nullptr, *dZ = nullptr;
+  cudaStream_t s = nullptr;
+  int phase = 0;                   // 0 created, 1 running, 2 ended, 3 finished
+  int info = 0;
+  long long steps = 0;
+  const jk_scorer *sc = nullptr;
+  jk_trace *trace = nullptr;       // the internal callers' trace (copied out by finish)
+  ~jk_solver()
+  {
+    if (exec) cudaGraphExecDestroy(exec);
+  }
+};
+
+namespace {
+
+int solver_make(jk_solver *v, int cplx, int n, const int *J, int n_2, int id_ncp, const jk_opts *opts,
+                const jk_trace *trace, const jk_scorer *sc)
+{
+  memset(&v->o, 0, sizeof(v->o));
+  if (opts) v->o = *opts;
+  v->n = n;
+  v->cplx = cplx;
+  v->n_2 = jstep_len(n, n_2);
+  v->sc = sc;
+  v->chunk = (v->o.graph_steps == 0) ? 32 : v->o.graph_steps;
+  Workspace &w = v->w;
+  Guard &g = v->g;
+  int rc = make_workspace(g, w, n, cplx, J, trace != nullptr, trace ? trace->max_steps : 0, trace ? trace->max_piv : 0);
   if (rc) return rc;
-  w.zba_quirk = (o.zba_quirk == 0) ? 1 : 0;
+  w.zba_quirk = (v->o.zba_quirk == 0) ? 1 : 0;
   w.id_ncp = id_ncp;
   if (id_ncp == 3) {
     const size_t nn = (size_t)n * (n - 1) / 2;
@@ -177,7 +196,7 @@ int run_loop(int cplx, int n, void *dU, void *dA, void *dZ, const int *J, double
     CK(cudaMemset(w.n3it, 0, sizeof(int)));
   }
   if (sc) {
-    // a learned solve: the scorer's device parameters, the off-norm buffers, the mode flags
+    // a learned solve: the scorer's device parameters, the off-norm buffers
     w.learned = 1;
     w.sc.w = sc->w;
     w.sc.b = sc->b;
@@ -185,61 +204,121 @@ int run_loop(int cplx, int n, void *dU, void *dA, void *dZ, const int *J, double
     CK(g.alloc(&w.offpart, kOffBlocks * sizeof(double)));
     CK(g.alloc(&w.offcount, sizeof(int)));
     CK(cudaMemset(w.offcount, 0, sizeof(int)));
-    State s1;
-    CK(cudaMemcpy(&s1, w.st, sizeof(State), cudaMemcpyDeviceToHost));
-    s1.learned = 1;
-    s1.stall_k = sc->stall_k;
-    CK(cudaMemcpy(w.st, &s1, sizeof(State), cudaMemcpyHostToDevice));
+    if (sc->nf == 0) {
+      // the Gram-guided ranking: the "+" x "-" column products and the column norms
+      CK(g.alloc(&w.gram, (size_t)w.n_plus * w.n_minus * sizeof(double)));
+      CK(g.alloc(&w.cn, (size_t)n * sizeof(double)));
+      CK(prepare_gram());
+    }
   }
+  return 0;
+}
 
-  g_launches = 2;  // state init, U = Z = I
-  CK(launch_init(w, dU, dZ, s));
-  int chunk = (o.graph_steps == 0) ? 32 : o.graph_steps;
-  cudaGraphExec_t exec = nullptr;
-  if (chunk > 0) {
-    // capture `chunk` whole steps once; if capture fails, fall back to plain stream launches
-    cudaGraph_t graph = nullptr;
-    cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
-    if (e == cudaSuccess) {
-      for (int k = 0; k < chunk && e == cudaSuccess; ++k) e = launch_step(w, dA, dU, dZ, n_2, s);
-      const cudaError_t e2 = cudaStreamEndCapture(s, &graph);
-      if (e == cudaSuccess) e = e2;
-    }
-    if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
-    if (graph) cudaGraphDestroy(graph);
-    if (e != cudaSuccess) {
-      cudaGetLastError();
-      if (exec) { cudaGraphExecDestroy(exec); exec = nullptr; }
-      chunk = -1;
-    }
+// kernel launches of one step of this solve
+long long step_launches(const Workspace &w)
+{
+  const bool hyp = (w.n_plus > 0 && w.n_minus > 0);
+  const int learned = !w.learned ? 0 : (!hyp ? 1 : (w.sc.nf == 0 ? 4 : 2));  // + the off-norm
+  return kStepLaunches - (hyp ? 0 : 1) + ((w.cplx && hyp) ? 1 : 0) + learned;
+}
+
+// a new solve (dsigma NULL), or the continuation of a loop that ended after steps0
+// steps with A, U, Z, SIGMA as its end left them
+int solver_start(jk_solver *v, void *dU, void *dA, void *dZ, const double *dsigma, long long steps0, cudaStream_t s)
+{
+  if (steps0 < 0 || steps0 > 0x7FFFFFFF) return -6;
+  v->dA = dA;
+  v->dU = dU;
+  v->dZ = dZ;
+  v->s = s;
+  v->phase = 1;
+  v->info = 0;
+  v->steps = steps0;
+  g_launches = 2;  // state init, U = Z = I (or the two kernels that undo the loop's end)
+  if (dsigma) CK(launch_unfinish(v->w, dA, dZ, dsigma, s));
+  CK(launch_init(v->w, dU, dZ, v->sc ? 1 : 0, v->sc ? v->sc->stall_k : 0, (int)steps0, dsigma ? 0 : 1, s));
+  if (v->w.n3it) CK(cudaMemsetAsync(v->w.n3it, 0, sizeof(int), s));
+  if (v->w.offcount) CK(cudaMemsetAsync(v->w.offcount, 0, sizeof(int), s));
+  return 0;
+}
+
+// capture `chunk` whole steps as a graph for the current buffers and stream; if capture
+// fails, the loop uses plain stream launches
+void solver_graph(jk_solver *v)
+{
+  const void *key[4] = { v->dA, v->dU, v->dZ, v->s };
+  if (v->chunk <= 0) return;
+  if (v->exec && !memcmp(key, v->key, sizeof(key))) return;
+  if (v->exec) { cudaGraphExecDestroy(v->exec); v->exec = nullptr; }
+  cudaGraph_t graph = nullptr;
+  cudaError_t e = cudaStreamBeginCapture(v->s, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    for (int k = 0; k < v->chunk && e == cudaSuccess; ++k) e = launch_step(v->w, v->dA, v->dU, v->dZ, v->n_2, v->s);
+    const cudaError_t e2 = cudaStreamEndCapture(v->s, &graph);
+    if (e == cudaSuccess) e = e2;
   }
-  const int per_sync = (chunk > 0) ? chunk : 32;
-  // a bound on the number of steps (the loop has none of its own)
-  const long long cap = (o.max_steps > 0) ? o.max_steps : (4000LL * n + 100000LL);
-  long long launched = 0;
-  int info = 0;
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&v->exec, graph, 0);
+  if (graph) cudaGraphDestroy(graph);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    if (v->exec) { cudaGraphExecDestroy(v->exec); v->exec = nullptr; }
+    v->chunk = -1;
+  }
+  memcpy(v->key, key, sizeof(key));
+}
+
+int solver_advance(jk_solver *v, long long k)
+{
+  if (v->phase == 0 || v->phase == 3) return JK_ERR_STATE;
+  if (v->phase == 2) return 1;
+  // the step count at which the loop waits: the caller's slice, capped by max_steps
+  long long target = (k > 0) ? v->steps + k : 0;
+  if (v->o.max_steps > 0 && (target == 0 || target > v->o.max_steps)) target = v->o.max_steps;
+  CK(launch_limit(v->w, target, v->s));
+  ++g_launches;
+  solver_graph(v);
+  const int per_sync = (v->chunk > 0) ? v->chunk : 32;
+  const long long per_step = step_launches(v->w);
+  long long last = v->steps;
+  int idle = 0;
   for (;;) {
     cudaError_t e = cudaSuccess;
-    if (exec) e = cudaGraphLaunch(exec, s);
+    if (v->exec) e = cudaGraphLaunch(v->exec, v->s);
     else
-      for (int k = 0; k < per_sync && e == cudaSuccess; ++k) e = launch_step(w, dA, dU, dZ, n_2, s);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(w.st_host, w.st, sizeof(State), cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    if (e != cudaSuccess) {
-      if (exec) cudaGraphExecDestroy(exec);
-      return cuda_fail(e);
+      for (int j = 0; j < per_sync && e == cudaSuccess; ++j) e = launch_step(v->w, v->dA, v->dU, v->dZ, v->n_2, v->s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(v->w.st_host, v->w.st, sizeof(State), cudaMemcpyDeviceToHost, v->s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(v->s);
+    if (e != cudaSuccess) return cuda_fail(e);
+    g_launches += (long long)per_sync * per_step;
+    const State &h = *v->w.st_host;
+    v->steps = h.steps;
+    if (h.stop == 1) { v->phase = 2; v->info = h.info; return 1; }
+    if (h.stop == 2) {
+      if (v->o.max_steps > 0 && v->steps >= v->o.max_steps) { v->phase = 2; v->info = JK_ERR_MAX_STEPS; return 1; }
+      return 0;
     }
-    launched += per_sync;
-    g_launches += (long long)per_sync * (kStepLaunches - ((w.n_plus > 0 && w.n_minus > 0) ? 0 : 1) +
-                                         ((w.cplx && w.n_plus > 0 && w.n_minus > 0) ? 1 : 0) +
-                                         (w.learned ? ((w.n_plus > 0 && w.n_minus > 0) ? 2 : 1) : 0));
-    if (w.st_host->stop) { info = w.st_host->info; break; }
-    if (w.st_host->steps >= cap || launched > 2 * cap + per_sync) { info = JK_ERR_MAX_STEPS; break; }
+    // every graph launch takes at least one step or ends the loop (a learned step
+    // without an effective pivot is followed by an exact one)
+    if (v->steps == last) {
+      if (++idle >= 3) return JK_ERR_STALL;
+    }
+    else { idle = 0; last = v->steps; }
   }
-  if (exec) cudaGraphExecDestroy(exec);
-  if (exact_steps) *exact_steps = w.st_host->exact_steps;
+}
+
+int solver_finish(jk_solver *v, double *dsigma, int *exact_steps)
+{
+  if (v->phase == 0 || v->phase == 3) return JK_ERR_STATE;
+  const int info = (v->phase == 2) ? v->info : JK_ERR_MAX_STEPS;
+  v->phase = 3;
+  cudaStream_t s = v->s;
+  Workspace &w = v->w;
   g_launches += 2;  // sigma, J Z^T J
-  CK(launch_finish(w, dA, dZ, dsigma, s));
+  CK(launch_finish(w, v->dA, v->dZ, dsigma, s));
+  CK(cudaMemcpyAsync(w.st_host, w.st, sizeof(State), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  if (exact_steps) *exact_steps = w.st_host->exact_steps;
+  jk_trace *trace = v->trace;
   if (trace) {
     const State &h = *w.st_host;
     const int ns = h.trace_steps < trace->max_steps ? h.trace_steps : trace->max_steps;
@@ -262,6 +341,21 @@ int run_loop(int cplx, int n, void *dU, void *dA, void *dZ, const int *J, double
   }
   CK(cudaStreamSynchronize(s));
   return info;
+}
+
+// the loop of DSTEP_LOOP / ZSTEP_LOOP on device buffers, in one call
+int run_loop(int cplx, int n, void *dU, void *dA, void *dZ, const int *J, double *dsigma, int n_2, int id_ncp, int id_tru,
+             const jk_opts *opts, jk_trace *trace, cudaStream_t s, const jk_scorer *sc = nullptr, int *exact_steps = nullptr)
+{
+  (void)id_tru;  // the pair order does not change the sorted records
+  jk_solver v;
+  int rc = solver_make(&v, cplx, n, J, n_2, id_ncp, opts, trace, sc);
+  if (rc) return rc;
+  v.trace = trace;
+  if ((rc = solver_start(&v, dU, dA, dZ, nullptr, 0, s))) return rc;
+  rc = solver_advance(&v, 0);
+  if (rc < 0) return rc;
+  return solver_finish(&v, dsigma, exact_steps);
 }
 
 int pick_device(const jk_opts *opts)
@@ -335,6 +429,55 @@ int jk_zstep_loop_dev(int n, double *dU, double *dA, double *dZ, const int *J, d
   const int rc = check_args(n, n, n, n, J, n_2, id_ncp, id_tru, 1);
   if (rc) return rc;
   return run_loop(1, n, dU, dA, dZ, J, dsigma, n_2, id_ncp, id_tru, opts, trace, (cudaStream_t)stream);
+}
+
+jk_solver *jk_solver_create(int n, int complex_, const int *J, int n_2, int id_ncp, int id_tru, const jk_opts *opts,
+                            int *info)
+{
+  const int cplx = complex_ ? 1 : 0;
+  int rc = check_args(n, n, n, n, J, n_2, id_ncp, id_tru, cplx);
+  jk_solver *v = nullptr;
+  if (!rc) {
+    v = new jk_solver;
+    rc = solver_make(v, cplx, n, J, n_2, id_ncp, opts, nullptr, nullptr);
+    if (rc) { delete v; v = nullptr; }
+  }
+  if (info) *info = rc;
+  return v;
+}
+
+void jk_solver_destroy(jk_solver *v) { delete v; }
+
+int jk_solver_begin(jk_solver *v, double *dU, double *dA, double *dZ, void *stream)
+{
+  if (!v) return -1;
+  if (!dU || !dA || !dZ) return -2;
+  return solver_start(v, dU, dA, dZ, nullptr, 0, (cudaStream_t)stream);
+}
+
+int jk_solver_resume(jk_solver *v, double *dU, double *dA, double *dZ, const double *dsigma, long long steps, void *stream)
+{
+  if (!v) return -1;
+  if (!dU || !dA || !dZ || !dsigma) return -2;
+  // a complex loop's end keeps only the real parts of the diagonal in SIGMA
+  if (v->cplx) return JK_ERR_STATE;
+  return solver_start(v, dU, dA, dZ, dsigma, steps, (cudaStream_t)stream);
+}
+
+int jk_solver_advance(jk_solver *v, long long steps)
+{
+  if (!v) return -1;
+  if (steps < 0) return -2;
+  return solver_advance(v, steps);
+}
+
+long long jk_solver_steps(const jk_solver *v) { return v ? v->steps : -1; }
+
+int jk_solver_finish(jk_solver *v, double *dsigma)
+{
+  if (!v) return -1;
+  if (!dsigma) return -2;
+  return solver_finish(v, dsigma, nullptr);
 }
 
 static int hsvd2_batch(int cplx, int count, double *A, const int *J, double *U, double *Z, int *info, double th1)
@@ -674,12 +817,18 @@ int jk_mlp_nparams(int nf) { return (nf == kMlpFeat) ? mlp_params(nf) : -1; }
 jk_scorer *jk_scorer_create(int nf, const float *params, int stall_k, int *info)
 {
   int rc = 0;
-  if (nf != kMlpFeat) rc = -1;
-  else if (!params) rc = -2;
+  if (nf != kMlpFeat && nf != 0) rc = -1;
+  else if (nf && !params) rc = -2;
   else if (stall_k < 1) rc = -3;
   if (!rc) rc = pick_device(nullptr);
   jk_scorer *sc = nullptr;
-  if (!rc) {
+  if (!rc && nf == 0) {
+    // the Gram-guided ranking: no network
+    sc = new jk_scorer;
+    sc->nf = 0;
+    sc->stall_k = stall_k;
+  }
+  else if (!rc) {
     sc = new jk_scorer;
     sc->nf = nf;
     sc->stall_k = stall_k;
@@ -795,6 +944,8 @@ const char *jk_strerror(int info)
   case JK_ERR_TOO_LARGE: return "N too large for this build";
   case JK_ERR_NO_DEVICE: return "no CUDA device";
   case JK_ERR_SCRATCH: return "N beyond the static scratch of jk_dweights_noalloc (JK_NOALLOC_MAX_N = 1024)";
+  case JK_ERR_STALL: return "internal: the device loop neither advanced nor ended";
+  case JK_ERR_STATE: return "a solver call out of order (or resume of a complex solve)";
   default: return "a 2x2 HSVD error (NaN or infinity in a pivot block) or argument error";
   }
 }

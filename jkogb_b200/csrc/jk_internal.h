@@ -10,7 +10,7 @@ namespace jk {
 // Loop state kept on the device (one per solve).  Mirrors the scalars of
 // DSTEP_LOOP / DSTEP_EXEC (src/D/dstep.F90:376-604).
 struct State {
-  int stop;    // 1 once the loop has ended
+  int stop;    // 1 once the loop has ended; 2 while it waits at `limit` (resumable)
   int steps;   // S: steps with effective transformations
   int info;    // final INFO (valid once stop)
   int sl;      // SL of the current step (selected pivots)
@@ -34,6 +34,7 @@ struct State {
   int exact_steps;   // steps run with the exact weights in a learned solve
   int retry;         // a learned step without an effective pivot: the loop goes on with an exact step
   double off, best_off;  // off-norm after the last step, its minimum so far
+  long long limit;   // the loop waits (stop = 2) once `steps` reaches this (0: never)
 };
 
 // Per-step trace on the device (optional).
@@ -83,8 +84,6 @@ struct Workspace {
   int *plus, *minus; // indices with J=+1 / J=-1, ascending
   double *Wm;        // n x n pair weights, symmetric, NaN = no transformation
   double *mag;       // complex: n x n magnitudes |A(i,j)| of the step
-  void *hpar;        // per hyperbolic pair: scan parameters (real path), 1024 slots per 32 x 32 tile
-  int *tcount;       // hyperbolic pairs per tile
   void *piv;         // Piv<T>[n/2]
   void *rowrot;      // RowRot<T>[n/2]
   unsigned short *list;  // n x list_ld(n): the partners of every vertex, best first
@@ -98,7 +97,9 @@ struct Workspace {
   double *offpart;   // per-block partial off-norms (learned solves)
   int *offcount;     // blocks done (the last one finishes the off-norm)
   int learned;       // rank the scanned hyperbolic pairs by `sc`
-  ScorerDev sc;
+  ScorerDev sc;      // sc.nf == 0: the Gram-guided ranking (no network)
+  double *gram;      // Gram-guided ranking: n_plus x n_minus off-diagonal column products
+  double *cn;        // ... and the columns' off-diagonal squared norms
   // ID_NCP = 3 (AW_NCP3): per record key and tie, the sorted order, every start's walk
   int id_ncp;
   unsigned long long *n3key;
@@ -109,7 +110,9 @@ struct Workspace {
 constexpr int kNcp3MaxN = 256;  // AW_NCP3's work grows as the square of the record count
 
 // host launchers (jk_kernels.cu)
-cudaError_t launch_init(Workspace &w, void *U, void *Z, cudaStream_t s);
+cudaError_t launch_init(Workspace &w, void *U, void *Z, int learned, int stall_k, int steps0, int fresh, cudaStream_t s);
+cudaError_t launch_unfinish(Workspace &w, void *A, void *Z, const double *sigma, cudaStream_t s);
+cudaError_t launch_limit(Workspace &w, long long limit, cudaStream_t s);
 cudaError_t launch_step(Workspace &w, void *A, void *U, void *Z, int n_2, cudaStream_t s);
 cudaError_t launch_finish(Workspace &w, void *A, void *Z, double *sigma, cudaStream_t s);
 cudaError_t launch_weights(Workspace &w, const void *A, cudaStream_t s);
@@ -139,6 +142,7 @@ constexpr int kMlpHidden = 64;
 constexpr int kMlpFeat = 7;
 __host__ __device__ constexpr int mlp_params(int nf) { return kMlpHidden * nf + kMlpHidden + kMlpHidden * kMlpHidden + kMlpHidden + kMlpHidden + 1; }
 cudaError_t launch_learned_weights(Workspace &w, const double *A, cudaStream_t s);
+cudaError_t prepare_gram();
 constexpr int kOffBlocks = 296;  // fixed grid of the off-norm reduction (a fixed summation order)
 cudaError_t launch_offnorm(Workspace &w, const double *A, cudaStream_t s);
 cudaError_t mlp_features(int n, const double *A, const int *plus, const int *minus, int n_plus, int n_minus, int step, int nf,

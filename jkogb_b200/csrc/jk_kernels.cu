@@ -45,21 +45,41 @@ __global__ void k_identity2(T *U, T *Z, int n)
   }
 }
 
-__global__ void k_state_init(State *st)
+// the loop state at the start of a solve (S = steps0; 0 for a new solve); the trace
+// capacities are kept, the learned-ranking settings are the caller's
+__global__ void k_state_init(State *st, int learned, int stall_k, int steps0)
 {
   const int cap_s = st->trace_cap_steps, on = st->trace_on;
   const long long cap_p = st->trace_cap_piv;
-  const int learned = st->learned, stall_k = st->stall_k;
   State z = {};
   z.trace_on = on;
   z.trace_cap_steps = cap_s;
   z.trace_cap_piv = cap_p;
   z.tw = -0.0;
+  z.steps = steps0;
   z.learned = learned;
   z.learned_step = learned;
   z.stall_k = stall_k;
   z.best_off = __longlong_as_double(0x7FF0000000000000LL);  // +inf
   *st = z;
+}
+
+// a new step limit; a loop waiting at the old one goes on
+__global__ void k_set_limit(State *st, long long limit)
+{
+  if (st->stop == 2) st->stop = 0;
+  st->limit = limit;
+}
+
+// A(i,i) := SIGMA(i): the loop's matrix back from what the end of the loop made of it
+template <typename T>
+__global__ void k_unsigma(T *A, const double *sigma, int n)
+{
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    T v = Tr<T>::zero();
+    *(double *)&v = sigma[i];
+    A[(long long)i * n + i] = v;
+  }
 }
 
 // SIGMA(S) = A(S,S); A(S,S) = 0   (src/D/dstep.F90:594-602, src/Z/zstep.F90:605-613)
@@ -209,6 +229,11 @@ __device__ __forceinline__ void cp_async8(void *smem, const void *gmem)
   const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem));
 }
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem)
+{
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem));
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
@@ -267,19 +292,21 @@ __device__ __forceinline__ void scan_chunk(const double *const *xs, const double
 
 // one sign-class tile: tile (ti, tj) holds the pairs of the "+" vertices
 // plus[32 ti .. 32 ti + 31] with the "-" vertices minus[32 tj .. 32 tj + 31], all of
-// them hyperbolic (up to 1024, 4 per thread).  First the 2x2 HSVDs of DMAGF2H (scan
-// parameters to this tile's slice of `par`, the other weights straight to W), then the
-// tile's 64 columns stream through a three-stage buffer in row chunks and every thread
-// runs its pairs' fma chains.  A warp whose pairs have none of their rows p, q in a
-// chunk runs that chunk without the per-row skip test.
+// them hyperbolic (up to 1024, 4 per thread).  First the 2x2 HSVDs of DMAGF2H (the scan
+// parameters of the pairs that need the column scan, compacted into shared memory that
+// the row buffer reuses once every thread holds its own pairs' parameters; the other
+// weights straight to W), then the tile's 64 columns stream through a three-stage
+// buffer in row chunks and every thread runs its pairs' fma chains.  A warp whose pairs
+// have none of their rows p, q in a chunk runs that chunk without the per-row skip test.
 __global__ void __launch_bounds__(SCAN_THREADS, 2)
 k_hyp_pm(const State *st, const double *__restrict__ A, const int *__restrict__ plus, const int *__restrict__ minus,
-         int n_plus, int n_minus, int n, double *__restrict__ Wm, HypPar *par)
+         int n_plus, int n_minus, int n, double *__restrict__ Wm)
 {
   if (st->stop || st->learned_step) return;  // a learned step ranks these pairs by the scorer
+  extern __shared__ __align__(16) unsigned char smem_raw[];
   const int TM = (n_minus + TW - 1) / TW;
   const int P0 = (blockIdx.x / TM) * TW, Q0 = (blockIdx.x % TM) * TW;
-  HypPar *tpar = par + (long long)blockIdx.x * (TW * TW);
+  HypPar *tpar = (HypPar *)smem_raw;  // [TW * TW], before the row buffer takes the space
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   __shared__ int s_cnt, s_warp[SCAN_THREADS / 32], s_col[2 * TW];
   if (tid < 2 * TW) {
@@ -325,7 +352,6 @@ k_hyp_pm(const State *st, const double *__restrict__ A, const int *__restrict__ 
   const int cnt = s_cnt;
   if (!cnt) return;
 
-  extern __shared__ __align__(16) unsigned char smem_raw[];
   double *buf = (double *)smem_raw;  // [SCAN_STAGES][2 * TW][SCAN_RS]: the "+" columns, then the "-" columns
   constexpr int K = 4, STAGE = 2 * TW * SCAN_RS;
   int pv[K], qv[K], cpq[K], fl[K];  // cpq: the tile columns of p (bits 0-7) and q (bits 8-15)
@@ -346,6 +372,7 @@ k_hyp_pm(const State *st, const double *__restrict__ A, const int *__restrict__ 
 #pragma unroll
   for (int k = 0; k < K; ++k)
     if (fl[k] & 1) { any = 1; if ((fl[k] & 6) != 6) fastv = 0; }
+  // (this barrier also ends every read of tpar before the row buffer overwrites it)
   if (!__syncthreads_or(any)) return;
   const bool allfast = __syncthreads_and(fastv);
   const int nchunk = (n + SCAN_ROWS - 1) / SCAN_ROWS;
@@ -856,12 +883,22 @@ __device__ void end_of_step(State *st, const Piv<T> *piv, const int *J, Trace &t
     if (st->retry) st->retry = 0;
     else { st->info = st->steps; st->stop = 1; }
   }
-  else st->steps += 1;
+  else {
+    st->steps += 1;
+    // the caller's step limit: the loop waits here, between two steps, and can go on
+    if (st->limit > 0 && st->steps >= st->limit) st->stop = 2;
+  }
 }
 
 // one block: the end of the previous step, the matching rounds, the ranking of the
 // matched pairs and the first N_2 of them (the pivots of this step, rank order),
-// and the columns outside the pivot set
+// and the columns outside the pivot set.
+// A round is two barriers: (A) every free vertex finds its best free partner, the first
+// free entry of its ranked list from its pointer on; (B) mutual proposals are matched.
+// Each vertex keeps a window of 16 list entries in shared memory, two 8-entry segments;
+// once its pointer leaves the first segment, the window slides by one segment and the
+// next segment is fetched with cp.async, which lands while the round's barriers pass.
+// A pointer that runs past the window falls back to synchronous loads.
 template <typename T>
 __global__ void __launch_bounds__(SEL_THREADS, 1)
 k_select(State *st, const double *__restrict__ Wm, const int *__restrict__ J, int n, int n_2,
@@ -873,12 +910,13 @@ k_select(State *st, const double *__restrict__ Wm, const int *__restrict__ J, in
   unsigned *stie = (unsigned *)(skey + s2);                   // [s2]
   int *sidx = (int *)(stie + s2);                             // [s2]
   int2 *pairs = (int2 *)(sidx + s2);                          // [n/2 + 1]
-  uint4 *win = (uint4 *)(pairs + (n / 2 + 1) + ((n / 2 + 1) & 1)); // [n]: 8 list entries from wbase
-  int *best = (int *)(win + n);                               // [n]
-  int *ptr = best + n;                                        // [n]
-  int *wbase = ptr + n;                                       // [n]
-  unsigned char *ms = (unsigned char *)(wbase + n);           // [n]
-  __shared__ int s_stop, s_cnt, s_got, s_nunp, s_rounds;
+  uint4 *win = (uint4 *)(pairs + (n / 2 + 1) + ((n / 2 + 1) & 1)); // [n][2]: list entries wbase .. wbase + 15
+  int *best = (int *)(win + 2 * n);                           // [n]
+  unsigned short *ptr = (unsigned short *)(best + n);         // [n]
+  unsigned short *wbase = ptr + n;                            // [n]
+  unsigned short *slen = wbase + n;                           // [n]
+  unsigned char *ms = (unsigned char *)(slen + n);            // [n]: 0 free, 1 matched, 2 retired
+  __shared__ int s_stop, s_cnt, s_nunp, s_rounds;
 
   const int tid = threadIdx.x, nth = blockDim.x, ld = list_ld(n);
   if (tid == 0) {
@@ -889,27 +927,32 @@ k_select(State *st, const double *__restrict__ Wm, const int *__restrict__ J, in
   __syncthreads();
   if (s_stop) return;
   for (int v = tid; v < n; v += nth) {
+    const uint4 *row = (const uint4 *)(list + (long long)v * ld);
+    const int L = len[v];
     ms[v] = 0;
     ptr[v] = 0;
     wbase[v] = 0;
-    win[v] = *(const uint4 *)(list + (long long)v * ld);
+    slen[v] = (unsigned short)L;
+    win[2 * v] = row[0];
+    if (L > 8) win[2 * v + 1] = row[1];
   }
   __syncthreads();
 
   for (int round = 0; round <= n / 2 + 1; ++round) {
-    // phase A: the best free partner, the first free entry of the ranked list; the
-    // 8 entries at wbase are kept in shared memory, later ones are loaded on demand
+    cp_async_wait<0>();  // this thread's window refills of the last round
+    // phase A: the best free partner of every free vertex
     for (int v = tid; v < n; v += nth) {
       if (ms[v]) continue;
-      int p = ptr[v];
-      const int L = len[v];
+      int p = ptr[v], wb = wbase[v];
+      const int L = slen[v];
       const unsigned short *row = list + (long long)v * ld;
       int found = -1;
       while (p < L && found < 0) {
-        const int a = p & ~7;
-        if (a == wbase[v]) {
-          const uint4 q4 = win[v];
+        if (p < wb + 16) {
+          const int sg = (p - wb) >> 3;
+          const uint4 q4 = win[2 * v + sg];
           const unsigned w4[4] = { q4.x, q4.y, q4.z, q4.w };
+          const int a = wb + 8 * sg;
 #pragma unroll
           for (int e = 0; e < 8; ++e) {
             const int idx = a + e;
@@ -920,6 +963,7 @@ k_select(State *st, const double *__restrict__ Wm, const int *__restrict__ J, in
           continue;
         }
         // past the window: fetch the next 32 entries with four independent loads
+        const int a = p & ~7;
         uint4 g4[4];
 #pragma unroll
         for (int j = 0; j < 4; ++j)
@@ -934,17 +978,31 @@ k_select(State *st, const double *__restrict__ Wm, const int *__restrict__ J, in
             const int u = (int)((w4[e >> 1] >> ((e & 1) * 16)) & 0xFFFFu);
             if (found < 0 && idx >= p && idx < L && !ms[u]) { found = u; p = idx; }
           }
-          if (found >= 0) { win[v] = g4[j]; wbase[v] = a + 8 * j; }
+          if (found >= 0) {
+            // the window restarts at the segment of the find
+            wb = a + 8 * j;
+            win[2 * v] = g4[j];
+            if (j < 3 && wb + 8 < L) win[2 * v + 1] = g4[j + 1];
+            else if (wb + 8 < L) cp_async16(&win[2 * v + 1], row + wb + 8);
+          }
         }
         if (found < 0) p = a + 32;
       }
       if (found < 0) p = L;
-      ptr[v] = p;
+      else if (p >= wb + 8 && p < wb + 16) {
+        // the first segment is used up: slide the window and fetch the segment after it
+        win[2 * v] = win[2 * v + 1];
+        wb += 8;
+        if (wb + 8 < L) cp_async16(&win[2 * v + 1], row + wb + 8);
+      }
+      cp_async_commit();
+      ptr[v] = (unsigned short)p;
+      wbase[v] = (unsigned short)wb;
       best[v] = found;
     }
-    if (tid == 0) { s_got = 0; s_rounds = round + 1; }
     __syncthreads();
     // phase B: mutual proposals are matched; a vertex without a candidate retires
+    int got = 0;
     for (int v = tid; v < n; v += nth) {
       if (ms[v]) continue;
       const int u = best[v];
@@ -953,14 +1011,13 @@ k_select(State *st, const double *__restrict__ Wm, const int *__restrict__ J, in
         ms[v] = 1;
         ms[u] = 1;
         pairs[atomicAdd(&s_cnt, 1)] = make_int2(v, u);
-        atomicAdd(&s_got, 1);
+        got = 1;
       }
     }
-    __syncthreads();
-    const int got = s_got;
-    __syncthreads();
-    if (!got) break;
+    if (tid == 0) s_rounds = round + 1;
+    if (!__syncthreads_or(got)) break;
   }
+  cp_async_wait<0>();
 
   // rank the matched pairs: (weight key, tie key), descending
   const int np = s_cnt;
@@ -1245,7 +1302,7 @@ size_t select_smem(int n)
 {
   const int s2 = pow2ceil(n / 2 > 0 ? n / 2 : 1);
   const int np = (n / 2 + 1) + ((n / 2 + 1) & 1);
-  return (size_t)s2 * (8 + 4 + 4) + (size_t)np * 8 + (size_t)n * (16 + 4 + 4 + 4 + 1) + 16;
+  return (size_t)s2 * (8 + 4 + 4) + (size_t)np * 8 + (size_t)n * (32 + 4 + 2 + 2 + 2 + 1) + 16;
 }
 
 // k_colsort instantiations: records per thread E = pow2ceil(n) / SORT_THREADS
@@ -1392,25 +1449,52 @@ cudaError_t prepare_kernels(int n)
 }
 
 template <typename T>
-static cudaError_t init_t(Workspace &w, T *U, T *Z, cudaStream_t s)
+static cudaError_t init_t(Workspace &w, T *U, T *Z, int learned, int stall_k, int steps0, int fresh, cudaStream_t s)
 {
-  k_state_init<<<1, 1, 0, s>>>(w.st);
-  k_identity2<T><<<grid1((long long)w.n * w.n, 256), 256, 0, s>>>(U, Z, w.n);
+  k_state_init<<<1, 1, 0, s>>>(w.st, learned, stall_k, steps0);
+  if (fresh) k_identity2<T><<<grid1((long long)w.n * w.n, 256), 256, 0, s>>>(U, Z, w.n);
   return cudaGetLastError();
 }
 
-cudaError_t launch_init(Workspace &w, void *U, void *Z, cudaStream_t s)
+// the loop state of a new solve (fresh: U = Z = I) or of a loop that went on for
+// steps0 steps (U, Z kept)
+cudaError_t launch_init(Workspace &w, void *U, void *Z, int learned, int stall_k, int steps0, int fresh, cudaStream_t s)
 {
-  return w.cplx ? init_t(w, (double2 *)U, (double2 *)Z, s) : init_t(w, (double *)U, (double *)Z, s);
+  return w.cplx ? init_t(w, (double2 *)U, (double2 *)Z, learned, stall_k, steps0, fresh, s)
+                : init_t(w, (double *)U, (double *)Z, learned, stall_k, steps0, fresh, s);
 }
+
+cudaError_t launch_limit(Workspace &w, long long limit, cudaStream_t s)
+{
+  k_set_limit<<<1, 1, 0, s>>>(w.st, limit);
+  return cudaGetLastError();
+}
+
+// undo the end of the loop (k_sigma, k_jztj): the diagonal back from SIGMA, and
+// J Z^T J again, which gives back Z (a transposition with sign changes)
+template <typename T>
+static cudaError_t unfinish_t(Workspace &w, T *A, T *Z, const double *sigma, cudaStream_t s)
+{
+  const int n = w.n, nt = (n + 31) / 32;
+  k_unsigma<T><<<grid1(n, 256), 256, 0, s>>>(A, sigma, n);
+  k_jztj<T><<<nt * (nt + 1) / 2, dim3(32, 8), 0, s>>>(Z, w.J, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_unfinish(Workspace &w, void *A, void *Z, const double *sigma, cudaStream_t s)
+{
+  return w.cplx ? unfinish_t(w, (double2 *)A, (double2 *)Z, sigma, s) : unfinish_t(w, (double *)A, (double *)Z, sigma, s);
+}
+
+// the row buffer, which also holds a tile's scan parameters before the rows arrive
+static_assert(TW * TW * sizeof(HypPar) <= SCAN_STAGES * (2 * TW) * SCAN_RS * sizeof(double),
+              "a tile's scan parameters must fit in the row buffer");
 
 static void hyp_d_launch(Workspace &w, const double *A, cudaStream_t s)
 {
-  // ceil(n_plus / 32) ceil(n_minus / 32) <= T (T + 1) / 2 tiles, T = ceil(n / 32): the
-  // parameter slices make_workspace allocates
   const int nt = ((w.n_plus + TW - 1) / TW) * ((w.n_minus + TW - 1) / TW);
   const size_t smem = SCAN_STAGES * (2 * TW) * SCAN_RS * sizeof(double);
-  k_hyp_pm<<<nt, SCAN_THREADS, smem, s>>>(w.st, A, w.plus, w.minus, w.n_plus, w.n_minus, w.n, w.Wm, (HypPar *)w.hpar);
+  k_hyp_pm<<<nt, SCAN_THREADS, smem, s>>>(w.st, A, w.plus, w.minus, w.n_plus, w.n_minus, w.n, w.Wm);
 }
 
 template <typename T>

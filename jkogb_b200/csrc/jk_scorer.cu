@@ -391,8 +391,11 @@ __global__ void k_mlp_pack(const float *__restrict__ P, unsigned short *w, float
 
 }  // namespace
 
+cudaError_t launch_gram_weights(Workspace &w, const double *A, cudaStream_t s);
+
 cudaError_t launch_learned_weights(Workspace &w, const double *A, cudaStream_t s)
 {
+  if (w.sc.nf == 0) return launch_gram_weights(w, A, s);  // the Gram-guided ranking, no network
   if (w.n_plus > 0 && w.n_minus > 0) {
     dim3 g((w.n_plus + 15) / 16, (w.n_minus + 15) / 16);
     k_hyp_learned<<<g, 256, 0, s>>>(w.st, A, w.plus, w.minus, w.n_plus, w.n_minus, w.Wm, w.n, w.sc);
@@ -454,6 +457,218 @@ cudaError_t mlp_pack(int nf, const float *params, unsigned short *w, float *b, c
   if (nf != NF) return cudaErrorInvalidValue;
   k_mlp_pack<<<(H * H + 255) / 256, 256, 0, s>>>(params, w, b);
   return cudaGetLastError();
+}
+
+}  // namespace jk
+
+namespace jk {
+
+// ---------------------------------------------------------------------------
+// The Gram-guided ranking.  A hyperbolic pair (p, q) that needs the column scan of
+// ABODNDF2 (src/D/dtransf.F90:246-348) has the weight
+//   d0 + sum_{i != p,q} (x_i^2 - x_i'^2) + (y_i^2 - y_i'^2),  x = A(:,p), y = A(:,q),
+// with x_i' = Z11 x_i + Z21 y_i, y_i' = Z12 x_i + Z22 y_i (Z2 the pair's 2x2 right
+// transformation).  The sum is, exactly in real arithmetic,
+//   nx (1 - Z11^2 - Z12^2) + ny (1 - Z21^2 - Z22^2) - 2 (Z11 Z21 + Z12 Z22) g
+// with nx = sum_{i != p,q} x_i^2, ny likewise and g = sum_{i != p,q} x_i y_i: a function of
+// three entries of the Gram matrix of A with its diagonal set to zero.  All of g for the
+// "+" x "-" pairs is one FP64 matrix product (k_gram, on the FP64 tensor pipe, DMMA);
+// nx, ny come from the columns' off-diagonal norms.  The result differs from the
+// reference's sequential sum only in rounding, so it ranks the pairs as the exact weight
+// does except between near-equal weights; the selection, the 2x2 HSVDs, the rotations and
+// the end-of-loop test stay exact.
+// ---------------------------------------------------------------------------
+
+// column off-diagonal norms cn[j] = sum_{i != j} A(i,j)^2 (one warp per column)
+__global__ void __launch_bounds__(256)
+k_colnorm(const State *st, const double *__restrict__ A, int n, double *__restrict__ cn)
+{
+  if (st->stop || !st->learned_step) return;
+  const int lane = threadIdx.x & 31;
+  for (int j = blockIdx.x * 8 + (threadIdx.x >> 5); j < n; j += gridDim.x * 8) {
+    const double *c = A + (long long)j * n;
+    double s = 0.0;
+    for (int i = lane; i < n; i += 32)
+      if (i != j) s = fma(c[i], c[i], s);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xFFFFFFFFu, s, o);
+    if (!lane) cn[j] = s;
+  }
+}
+
+// G[a][b] = sum_i A0(i, plus[a]) A0(i, minus[b]) with A0 = A minus its diagonal:
+// a 64 x 64 tile per block of 4 warps (32 x 32 each, 4 x 4 DMMA m8n8k4 tiles), row
+// chunks of 32 staged with cp.async in two buffers; the diagonal entries are masked
+// when the fragments are read.
+#define GT 64
+#define GK 32
+#define GKP 36  // padded chunk row: the 8 x 4 fragment reads hit distinct banks
+constexpr size_t kGramOperand = 2 * GT * GKP * sizeof(double);  // one operand's two buffers
+
+__device__ __forceinline__ void dmma_8x8x4(double (&c)[2], double a, double b)
+{
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+               : "+d"(c[0]), "+d"(c[1])
+               : "d"(a), "d"(b));
+}
+
+__device__ __forceinline__ void cp_async16g(void *smem, const void *gmem, bool full)
+{
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  const int sz = full ? 16 : 0;  // 0: the 16 bytes are zero-filled
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(gmem), "r"(sz));
+}
+
+__global__ void __launch_bounds__(128)
+k_gram(const State *st, const double *__restrict__ A, const int *__restrict__ plus, const int *__restrict__ minus,
+       int n_plus, int n_minus, int n, double *__restrict__ G)
+{
+  if (st->stop || !st->learned_step) return;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double (*xs)[GT][GKP] = (double (*)[GT][GKP])smem_raw;            // [2][GT][GKP]
+  double (*ys)[GT][GKP] = (double (*)[GT][GKP])(smem_raw + kGramOperand);
+  __shared__ int cx[GT], cy[GT];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int a0 = blockIdx.x * GT, b0 = blockIdx.y * GT;
+  if (tid < GT) {
+    cx[tid] = (a0 + tid < n_plus) ? plus[a0 + tid] : -1;
+    cy[tid] = (b0 + tid < n_minus) ? minus[b0 + tid] : -1;
+  }
+  __syncthreads();
+  const int nk = (n + GK - 1) / GK;
+  // staging: 2 operands x 64 columns x 16 pieces of 16 bytes (two rows each) = 2048
+  // copies, 16 per thread; a piece that is not 16-byte aligned in A or runs past row n
+  // is loaded by plain loads (zeros past the end)
+  auto stage = [&](int c) {
+    if (c < nk) {
+      const int k0 = c * GK, buf = c & 1;
+#pragma unroll
+      for (int t = 0; t < 16; ++t) {
+        const int idx = tid + 128 * t;        // 0 .. 2047
+        const int op = idx >> 10, col = (idx >> 4) & 63, piece = idx & 15;
+        const int g = op ? cy[col] : cx[col];
+        const int r = k0 + 2 * piece;
+        double *dst = op ? &ys[buf][col][2 * piece] : &xs[buf][col][2 * piece];
+        const long long e = (long long)g * n + r;
+        if (g >= 0 && r + 1 < n && !(e & 1)) cp_async16g(dst, A + e, true);  // 16-byte aligned piece
+        else {
+          dst[0] = (g >= 0 && r < n) ? A[e] : 0.0;
+          dst[1] = (g >= 0 && r + 1 < n) ? A[e + 1] : 0.0;
+        }
+      }
+    }
+    asm volatile("cp.async.commit_group;\n" ::);
+  };
+  double acc[4][4][2];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+  const int wm = (warp & 1) * 32, wn = (warp >> 1) * 32;  // the warp's 32 x 32 sub-tile
+  const int fr = lane >> 2, fk = lane & 3;                   // fragment row / k of this lane
+  int gxa[4], gyb[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) { gxa[i] = cx[wm + 8 * i + fr]; gyb[i] = cy[wn + 8 * i + fr]; }
+  stage(0);
+  for (int c = 0; c < nk; ++c) {
+    stage(c + 1);
+    asm volatile("cp.async.wait_group 1;\n" ::);
+    __syncthreads();
+    const int buf = c & 1, k0 = c * GK;
+#pragma unroll
+    for (int kk = 0; kk < GK; kk += 4) {
+      const int row = k0 + kk + fk;  // the matrix row this lane's fragments hold
+      double fa[4], fb[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        fa[i] = (row == gxa[i]) ? 0.0 : xs[buf][wm + 8 * i + fr][kk + fk];
+        fb[i] = (row == gyb[i]) ? 0.0 : ys[buf][wn + 8 * i + fr][kk + fk];
+      }
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) dmma_8x8x4(acc[i][j], fa[i], fb[j]);
+    }
+    __syncthreads();
+  }
+  asm volatile("cp.async.wait_group 0;\n" ::);
+  // C fragment: row fr, columns 2 fk, 2 fk + 1 of each 8 x 8 tile
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int a = a0 + wm + 8 * i + fr;
+    if (a >= n_plus) continue;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int b = b0 + wn + 8 * j + 2 * fk;
+      if (b < n_minus) G[(long long)a * n_minus + b] = acc[i][j][0];
+      if (b + 1 < n_minus) G[(long long)a * n_minus + b + 1] = acc[i][j][1];
+    }
+  }
+}
+
+
+// the weights of the hyperbolic pairs of a Gram-guided step: the 2x2 part of DMAGF2H
+// exact (src/D/dstep.F90:41-72), the scanned part from the Gram entries
+__global__ void __launch_bounds__(256)
+k_hyp_gram(const State *st, const double *__restrict__ A, const int *__restrict__ plus, const int *__restrict__ minus,
+           int n_plus, int n_minus, int n, const double *__restrict__ G, const double *__restrict__ cn,
+           double *__restrict__ Wm)
+{
+  if (st->stop || !st->learned_step) return;
+  const long long k = blockIdx.x * 256LL + threadIdx.x;
+  if (k >= (long long)n_plus * n_minus) return;
+  const int ia = (int)(k / n_minus), ib = (int)(k % n_minus);
+  const int a = plus[ia], b = minus[ib];
+  const bool a_is_p = a < b;
+  const int p = a_is_p ? a : b, q = a_is_p ? b : a;
+  const double app = A[(long long)p * n + p], aqp = A[(long long)p * n + q], apq = A[(long long)q * n + p],
+               aqq = A[(long long)q * n + q];
+  double w = nan_w();
+  if (may_transform(app, aqp, apq, aqq)) {
+    double A2[4] = { app, aqp, apq, aqq }, U2[4], Z2[4];
+    int info = 0;
+    const int jp = a_is_p ? 1 : -1;
+    dhsvd2(A2, jp, -jp, U2, Z2, JK_TH1FIX, info);
+    if (info < 0) w = nan_w();
+    else if (!(info & 1)) w = 0.0;
+    else if (!(info & 4)) w = dasum2(aqp, apq);
+    else {
+      const double a1 = (info & 8) ? A2[M21] : 0.0, a2 = (info & 8) ? A2[M12] : 0.0;
+      double d = 0.0;
+      d = fma(__dsub_rn(aqp, a1), __dadd_rn(aqp, a1), d);
+      d = fma(__dsub_rn(apq, a2), __dadd_rn(apq, a2), d);
+      const double z11 = Z2[M11], z21 = Z2[M21], z12 = Z2[M12], z22 = Z2[M22];
+      const double nx = cn[p] - aqp * aqp, ny = cn[q] - apq * apq;
+      const double g = G[(long long)ia * n_minus + ib];
+      // 1 - z11^2 - z12^2 and 1 - z21^2 - z22^2 without cancellation at z11, z22 near +-1
+      const double c1 = (1.0 - z11) * (1.0 + z11) - z12 * z12;
+      const double c2 = (1.0 - z22) * (1.0 + z22) - z21 * z21;
+      const double c3 = z11 * z21 + z12 * z22;
+      w = d + (nx * c1 + ny * c2 - 2.0 * c3 * g);
+    }
+  }
+  if (w < -JK_HUGE) w = nan_w();
+  Wm[(long long)q * n + p] = w;
+  Wm[(long long)p * n + q] = w;
+}
+
+cudaError_t launch_gram_weights(Workspace &w, const double *A, cudaStream_t s)
+{
+  if (w.n_plus > 0 && w.n_minus > 0) {
+    const int n = w.n;
+    k_colnorm<<<(n + 7) / 8 < 1184 ? (n + 7) / 8 : 1184, 256, 0, s>>>(w.st, A, n, w.cn);
+    dim3 g((w.n_plus + GT - 1) / GT, (w.n_minus + GT - 1) / GT);
+    k_gram<<<g, 128, 2 * kGramOperand, s>>>(w.st, A, w.plus, w.minus, w.n_plus, w.n_minus, n, w.gram);
+    const long long np = (long long)w.n_plus * w.n_minus;
+    k_hyp_gram<<<(unsigned)((np + 255) / 256), 256, 0, s>>>(w.st, A, w.plus, w.minus, w.n_plus, w.n_minus, n, w.gram,
+                                                           w.cn, w.Wm);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t prepare_gram()
+{
+  return cudaFuncSetAttribute(k_gram, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(2 * kGramOperand));
 }
 
 }  // namespace jk

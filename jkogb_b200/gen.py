@@ -97,6 +97,23 @@ def prescribed(sigma, J, seed: int = 6, rotations: int | None = None, t_max: flo
     return np.asfortranarray(Q @ (sigma[:, None] * H))
 
 
+def prescribed_graded(n: int, lo: float, seed: int = 8) -> tuple[np.ndarray, np.ndarray]:
+    """A matrix with prescribed hyperbolic singular values log-uniform in [lo, 1] (the
+    grading of the graded workloads), J with n/2 entries of each sign in a seeded
+    permutation; built by prescribed().  Returns (Y, J); the prescribed values are
+    prescribed_graded_sigma(n, lo, seed)."""
+    sig, J = prescribed_graded_sigma(n, lo, seed)
+    return prescribed(sig, J, seed=seed + 1000), J
+
+
+def prescribed_graded_sigma(n: int, lo: float, seed: int = 8) -> tuple[np.ndarray, np.ndarray]:
+    """The prescribed values and J of prescribed_graded."""
+    r = _rng(seed)
+    sig = np.exp(r.uniform(np.log(lo), 0.0, n))
+    J = np.concatenate([np.ones(n // 2, np.int64), -np.ones(n - n // 2, np.int64)])[r.permutation(n)]
+    return sig, J
+
+
 # The five workloads of the benchmark plan, by name.
 WORKLOADS = {
     "djk_n256": dict(kind="real", n=256, n_2=128, make=lambda: gaussian(256, seed=1, n_plus=192)),

@@ -159,14 +159,19 @@ def train(X, T, params=None, iters=2000, batch=8192, lr=2e-3, seed=0, log=None):
 
 
 class Scorer:
-    """A trained network on the device (jk_scorer_create)."""
+    """A ranking for the scored solve (jk_scorer_create): a trained network (params), or,
+    with params None, the Gram-guided ranking (the scanned weights from the Gram matrix
+    of the off-diagonal columns, no network)."""
 
-    def __init__(self, params, stall_k=8):
-        p = np.ascontiguousarray(np.asarray(params, np.float32))
-        if p.size != nparams():
-            raise ValueError(f"expected {nparams()} parameters")
+    def __init__(self, params=None, stall_k=8):
         info = C.c_int(0)
-        self._s = lib().jk_scorer_create(NF, p.ctypes.data_as(C.POINTER(C.c_float)), int(stall_k), C.byref(info))
+        if params is None:
+            self._s = lib().jk_scorer_create(0, None, int(stall_k), C.byref(info))
+        else:
+            p = np.ascontiguousarray(np.asarray(params, np.float32))
+            if p.size != nparams():
+                raise ValueError(f"expected {nparams()} parameters")
+            self._s = lib().jk_scorer_create(NF, p.ctypes.data_as(C.POINTER(C.c_float)), int(stall_k), C.byref(info))
         if not self._s:
             raise JkError(info.value, "scorer: ")
 

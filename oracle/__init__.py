@@ -62,6 +62,10 @@ def lib():
         L.jo_tru2.argtypes = [C.c_int, ip, C.c_int, ip, ip, ip]
         L.jo_jstep_len.restype = C.c_int
         L.jo_jstep_len.argtypes = [C.c_int, C.c_int]
+        for nm in ("jq_dsigma_q", "jq_dsigma_ld", "jq_zsigma_q", "jq_zsigma_ld"):
+            f = getattr(L, nm)
+            f.restype = C.c_int
+            f.argtypes = [C.c_int, dp, C.c_int, ip, dp, C.c_int, C.c_int]
         L.jo_set_zba_quirk.argtypes = [C.c_int]
         L.jo_set_max_steps.argtypes = [C.c_int]
         _lib = L
@@ -132,6 +136,37 @@ def step_loop(Y, J, n_2=0, id_ncp=0, id_tru=0, nt=1, trace=False, max_steps=1 <<
     if trace:
         out["trace"] = _collect(trp, bufs)
     return out
+
+
+def accurate_sigma(Y, J, precision="q", nt=None, max_sweeps=60):
+    """The accuracy oracle (jk_accuracy.c): the hyperbolic singular values of Y with
+    signature J by one-sided hyperbolic Jacobi in __float128 ("q") or long double ("ld"),
+    rounded to float64; sigma[i] is attached to J[i] (compare within each sign class,
+    sorted).  Returns (sigma, sweeps)."""
+    Y = np.asarray(Y)
+    n = Y.shape[0]
+    cplx = np.iscomplexobj(Y)
+    A = np.asfortranarray(Y.astype(np.complex128 if cplx else np.float64))
+    Jc = np.ascontiguousarray(np.asarray(J).astype(np.int32))
+    s = np.zeros(n, np.float64)
+    nt = nt or (os.cpu_count() or 1)
+    fn = getattr(lib(), f"jq_{'z' if cplx else 'd'}sigma_{precision}")
+    sw = fn(n, _dp(A), n, _ip(Jc), _dp(s), int(nt), int(max_sweeps))
+    if sw < 0:
+        raise RuntimeError(f"the accuracy oracle did not converge ({sw})")
+    return s, sw
+
+
+def sigma_rel_err(sigma, ref, J):
+    """Max relative error of sigma against ref, within each J sign class (both sorted)."""
+    J = np.asarray(J)
+    err = 0.0
+    for c in (1, -1):
+        m = J == c
+        if m.any():
+            a, b = np.sort(np.asarray(sigma)[m]), np.sort(np.asarray(ref)[m])
+            err = max(err, float(np.max(np.abs(a - b) / np.abs(b))))
+    return err
 
 
 def hsvd2(A2, J2, th1=0.75):

@@ -8,8 +8,9 @@
 # wpqb.c keeps its selection count in the padding bytes of an 80-bit long double
 # (a union) and then stores to the long double; an optimising build may drop the
 # last count increment as a dead store, so the alt library is built at -O0.
-# Usage: make -f ref.mk [REF=/path/to/reference]
-REF ?= /root/reference
+# Usage: make -f ref.mk [REF=path/to/the/reference/checkout]
+# By default the checkout is the repository's sibling directory `reference`.
+REF ?= $(abspath $(CURDIR)/../../reference)
 OUT := _ref
 CC := gcc
 CFLAGS := -std=gnu18 -fno-strict-aliasing -fPIC -shared -D_GNU_SOURCE -w

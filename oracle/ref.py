@@ -19,7 +19,8 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _ALT = os.path.join(_HERE, "_ref", "libjkref_alt.so")
 _VAR = os.path.join(_HERE, "_ref", "libjkref_var.so")
-REF_ROOT = os.environ.get("JKOGB_REFERENCE", "/root/reference")
+# the reference checkout: $JKOGB_REFERENCE, else the repository's sibling directory `reference`
+REF_ROOT = os.environ.get("JKOGB_REFERENCE", os.path.normpath(os.path.join(_HERE, "..", "..", "reference")))
 
 
 def build() -> bool:

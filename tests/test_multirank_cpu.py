@@ -1,6 +1,8 @@
-"""The multi-rank plumbing of the benchmark on CPU: two gloo ranks over 127.0.0.1.  The
-job's time is the maximum over ranks, and the batched workload gives every rank its own
-batch (the ranks partition the job; no collective touches the data)."""
+"""The multi-rank paths on CPU: gloo ranks over 127.0.0.1.  The job's time is the maximum
+over ranks; one batch of matrices is partitioned over the ranks by estimated cost (the
+longest-processing-time rule on N^4), each rank solves its share and rank 0 gathers the
+per-matrix results back into the batch's order.  The ranks solve with the oracle here,
+so the test needs no GPU."""
 import os
 import socket
 
@@ -16,31 +18,60 @@ def _free_port():
     return p
 
 
+def _oracle_solve(mats, Js):
+    import oracle
+    out = []
+    for Y, J in zip(mats, Js):
+        r = oracle.step_loop(Y, J, nt=1)
+        out.append((int(r["info"]), r["sigma"].copy()))
+    return out
+
+
 def _rank(rank, world, port, out):
     from datetime import timedelta
 
     import torch.distributed as dist
 
     import bench
-    from jkogb_b200 import gen
+    from jkogb_b200 import gen, partition
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world))
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=60))
     t = bench.max_over_ranks(10.0 * rank + 1.0)
-    b = gen.batch(3, 16, 32, seed=bench.rank_batch_seed(rank))
-    out[rank] = (t, float(np.sum(b[0][0])))
+    b = gen.batch(9, 8, 24, seed=11)
+    res, share = partition.solve_partitioned([Y for Y, _ in b], [J for _, J in b], _oracle_solve)
+    out[rank] = (t, [int(i) for i in share], res)
     dist.barrier()
     dist.destroy_process_group()
 
 
-def test_two_gloo_ranks_time_and_partition():
+def test_two_gloo_ranks_partitioned_batch():
     world = 2
     port = _free_port()
     with mp.Manager() as m:
         out = m.dict()
         mp.spawn(_rank, args=(world, port, out), nprocs=world, join=True)
         res = dict(out)
-    assert res[0][0] == res[1][0] == 11.0      # the slowest rank's time on every rank
-    assert res[0][1] != res[1][1]              # different batches on different ranks
+    assert res[0][0] == res[1][0] == 11.0            # the slowest rank's time on every rank
+    s0, s1 = set(res[0][1]), set(res[1][1])
+    assert s0 and s1 and not (s0 & s1) and (s0 | s1) == set(range(9))  # disjoint shares, the whole batch
+    assert res[1][2] is None                         # only rank 0 gathers
+    from jkogb_b200 import gen
+    b = gen.batch(9, 8, 24, seed=11)
+    direct = _oracle_solve([Y for Y, _ in b], [J for _, J in b])
+    got = res[0][2]
+    assert len(got) == 9
+    for (i1, s1_), (i2, s2_) in zip(got, direct):   # the batch's order, the results of solving each alone
+        assert i1 == i2 and np.array_equal(s1_, s2_)
+
+
+def test_partition_balance_on_the_batch_workload():
+    from jkogb_b200 import gen, partition
+    ns = [Y.shape[0] for Y, _ in gen.batch(4096, 16, 128, seed=4)]
+    for world in (1, 2, 4, 8):
+        shares = partition.partition(ns, world)
+        allidx = np.concatenate(shares)
+        assert np.array_equal(np.sort(allidx), np.arange(len(ns)))   # every matrix exactly once
+        assert partition.imbalance(shares, ns) < 1.002                # estimated costs within 0.2%
 
 
 def test_single_process_max_is_identity():
