@@ -184,39 +184,47 @@ int jk_batch_tune(jk_batch *b, const double *dA, double *dU, double *dZ, double 
 int jk_dstep_loop_batched(int count, const int *n, const int *n_2, double *A, double *U, double *Z, const int *J,
                           double *sigma, int *info, const jk_opts *opts);
 
-/* The learned ranking (no counterpart in the reference's code; it follows the plan of
- * a learned pivot scorer beside the exact method).  A scorer is a network
- * 7 -> 64 -> 64 -> 1 (ReLU, BF16 weights, FP32 biases and accumulation) that predicts
- * a hyperbolic pair's weight (DMAGF2H, src/D/dstep.F90:41-72) from the pair's 2x2 block:
- * features log2|A(p,q)|/64, log2|A(q,p)|/64, log2|A(p,p)|/64, log2|A(q,q)|/64, J(p),
- * J(q), min(S / (10 N), 4); target g(w) = sign(w) (log2|w| + 1100) / 1024, g(0) = 0.
- * In a scored solve it replaces, for ranking only, the weights that need the O(N)
- * column scan; the NaN tests, the other weights, the selection, the 2x2 HSVDs and the
- * rotations stay exact.  Only a step ranked by the exact weights can end the loop (a
- * learned step without an effective pivot is followed by an exact step), and a step
- * whose off-norm has not reached a new minimum for `stall_k` steps is followed by an
- * exact step; once the off-norm exceeds 16 times its minimum, the rest of the solve
- * ranks exactly.
- * Parameters (floats, FP32 master copy): W1 [64][7] (row-major), b1 [64], W2 [64][64],
- * b2 [64], W3 [64], b3: jk_mlp_nparams(7) = 4737 floats. */
-#define JK_MLP_FEATURES 7
+/* The learned ranking (no counterpart in the reference, which ranks by the exact weights
+ * of DMAGF2H, src/D/dstep.F90:41-72).  In a scored step the hyperbolic pairs that need the
+ * O(N) column scan of ABODNDF2 (src/D/dtransf.F90:246-348) are ranked by
+ *   w_gram  the same off-norm reduction written through the Gram matrix of the columns
+ *           without their diagonal (one FP64 matrix product per step on the FP64 tensor
+ *           pipe) and the pair's exact 2x2 transformation; it equals the exact weight up
+ *           to rounding, and
+ *   w       = w_gram * 2^(clamp(y, -1, 1) / 8), y the output of a network
+ *           8 -> 64 -> 64 -> 1 (ReLU, BF16 weights and inputs, FP32 biases and
+ *           accumulation, on the tensor cores) that learns the correction from
+ *           features: log2/64 of |w_gram|, the two columns' squared off-norms without rows
+ *           p, q, |their product|, |the two leading terms|, |Z12| + |Z21|; sign(w_gram);
+ *           min(S / (10 N), 4).  Training target: clamp(8 log2(w / w_gram), -1, 1) with w the
+ *           exact weight (0 when the signs differ).
+ * The NaN tests, the other weights, the selection, the 2x2 HSVDs and the rotations stay
+ * exact.  Only a step ranked by the exact weights can end the loop (a scored step without
+ * an effective pivot is followed by an exact step), a step whose off-norm has not reached
+ * a new minimum for `stall_k` steps is followed by an exact step, and once the off-norm
+ * exceeds 16 times its minimum the rest of the solve ranks exactly.
+ * Parameters (floats, FP32 master copy): W1 [64][8] (row-major), b1 [64], W2 [64][64],
+ * b2 [64], W3 [64], b3: jk_mlp_nparams(8) = 4801 floats.  jk_scorer_create with nf = 0 and
+ * params NULL ranks by w_gram alone (no network). */
+#define JK_MLP_FEATURES 8
 typedef struct jk_scorer jk_scorer;
 int jk_mlp_nparams(int nf);
 jk_scorer *jk_scorer_create(int nf, const float *params, int stall_k, int *info);
 void jk_scorer_destroy(jk_scorer *sc);
-/* jk_dstep_loop_dev with the scorer ranking; *exact_steps (optional) receives the steps
+/* jk_dstep_loop_dev with the scored ranking; *exact_steps (optional) receives the steps
  * that ranked by the exact weights. */
 int jk_dstep_loop_dev_scored(int n, double *dU, double *dA, double *dZ, const int *J, double *dsigma, int n_2,
                              const jk_scorer *sc, const jk_opts *opts, jk_trace *trace, int *exact_steps, void *stream);
 /* Training on the device.  jk_mlp_features writes the features of every hyperbolic pair
  * of the device matrix dA (step S = `step`) in (+ index, - index) order, the indices
- * ascending within each sign class, and returns their count.  jk_mlp_forward: the
- * network (weights rounded to BF16) on `count` feature rows.  jk_mlp_grad: mean
- * squared error against dT and its gradient with respect to the FP32 parameters
- * (weights used rounded to BF16), summed in a fixed order; dWork holds
+ * ascending within each sign class, and returns their count; dWg (optional) receives each
+ * pair's w_gram, NaN for the pairs that need no column scan (their features are zero).
+ * jk_mlp_forward: the network (the inference arithmetic) on `count` feature rows.
+ * jk_mlp_grad: mean squared error against dT and its gradient with respect to the FP32
+ * parameters (weights used rounded to BF16), summed in a fixed order; dWork holds
  * jk_mlp_grad_workspace(nf, count) floats.  jk_mlp_adam: one Adam update of the
  * parameters (step t >= 1). */
-long long jk_mlp_features(int n, const double *dA, const int *J, int step, float *dX, void *stream);
+long long jk_mlp_features(int n, const double *dA, const int *J, int step, float *dX, double *dWg, void *stream);
 int jk_mlp_forward(int nf, int count, const float *dX, const float *dParams, float *dY, void *stream);
 long long jk_mlp_grad_workspace(int nf, int count);
 int jk_mlp_grad(int nf, int count, const float *dX, const float *dT, const float *dParams, float *dGrad, float *dLoss,

@@ -129,7 +129,7 @@ def lib():
         L.jk_dstep_loop_dev_scored.argtypes = [C.c_int, vp, vp, vp, ip, vp, C.c_int, C.c_void_p, C.POINTER(Opts),
                                                C.POINTER(Trace), ip, vp]
         L.jk_mlp_features.restype = C.c_longlong
-        L.jk_mlp_features.argtypes = [C.c_int, vp, ip, C.c_int, vp, vp]
+        L.jk_mlp_features.argtypes = [C.c_int, vp, ip, C.c_int, vp, vp, vp]
         L.jk_mlp_forward.restype = C.c_int
         L.jk_mlp_forward.argtypes = [C.c_int, C.c_int, vp, vp, vp, vp]
         L.jk_mlp_grad_workspace.restype = C.c_longlong

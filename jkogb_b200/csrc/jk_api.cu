@@ -204,12 +204,10 @@ int solver_make(jk_solver *v, int cplx, int n, const int *J, int n_2, int id_ncp
     CK(g.alloc(&w.offpart, kOffBlocks * sizeof(double)));
     CK(g.alloc(&w.offcount, sizeof(int)));
     CK(cudaMemset(w.offcount, 0, sizeof(int)));
-    if (sc->nf == 0) {
-      // the Gram-guided ranking: the "+" x "-" column products and the column norms
-      CK(g.alloc(&w.gram, (size_t)w.n_plus * w.n_minus * sizeof(double)));
-      CK(g.alloc(&w.cn, (size_t)n * sizeof(double)));
-      CK(prepare_gram());
-    }
+    // the Gram form of the scanned weights: the "+" x "-" column products, the column norms
+    CK(g.alloc(&w.gram, ((size_t)w.n_plus * w.n_minus + 1) * sizeof(double)));
+    CK(g.alloc(&w.cn, (size_t)n * sizeof(double)));
+    CK(prepare_gram());
   }
   return 0;
 }
@@ -218,7 +216,7 @@ int solver_make(jk_solver *v, int cplx, int n, const int *J, int n_2, int id_ncp
 long long step_launches(const Workspace &w)
 {
   const bool hyp = (w.n_plus > 0 && w.n_minus > 0);
-  const int learned = !w.learned ? 0 : (!hyp ? 1 : (w.sc.nf == 0 ? 4 : 2));  // + the off-norm
+  const int learned = !w.learned ? 0 : (hyp ? 4 : 1);  // norms, Gram, weights; the off-norm
   return kStepLaunches - (hyp ? 0 : 1) + ((w.cplx && hyp) ? 1 : 0) + learned;
 }
 
@@ -858,7 +856,7 @@ int jk_dstep_loop_dev_scored(int n, double *dU, double *dA, double *dZ, const in
   return run_loop(0, n, dU, dA, dZ, J, dsigma, n_2, 0, 0, opts, trace, (cudaStream_t)stream, sc, exact_steps);
 }
 
-long long jk_mlp_features(int n, const double *dA, const int *J, int step, float *dX, void *stream)
+long long jk_mlp_features(int n, const double *dA, const int *J, int step, float *dX, double *dWg, void *stream)
 {
   if (n < 3 || !dA || !J || !dX) return -1;
   std::vector<int> plus, minus;
@@ -871,13 +869,22 @@ long long jk_mlp_features(int n, const double *dA, const int *J, int step, float
   if (!cnt) return 0;
   Guard g;
   int *dp = nullptr, *dm = nullptr;
+  double *G = nullptr, *cn = nullptr;
+  State *st = nullptr;
   cudaStream_t s = (cudaStream_t)stream;
   CK(g.alloc(&dp, plus.size() * sizeof(int)));
   CK(g.alloc(&dm, minus.size() * sizeof(int)));
+  CK(g.alloc(&G, cnt * sizeof(double)));
+  CK(g.alloc(&cn, n * sizeof(double)));
+  CK(g.alloc(&st, sizeof(State)));
+  State s0;
+  memset(&s0, 0, sizeof(s0));
+  s0.learned = s0.learned_step = 1;  // the Gram kernels run in scored steps only
+  CK(cudaMemcpy(st, &s0, sizeof(State), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(dp, plus.data(), plus.size() * sizeof(int), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(dm, minus.data(), minus.size() * sizeof(int), cudaMemcpyHostToDevice));
-  CK(mlp_features(n, dA, dp, dm, (int)plus.size(), (int)minus.size(), step, kMlpFeat, dX, s));
-  CK(cudaStreamSynchronize(s));  // the index lists are freed on return
+  CK(mlp_features(n, dA, dp, dm, (int)plus.size(), (int)minus.size(), step, st, G, cn, dX, dWg, s));
+  CK(cudaStreamSynchronize(s));  // the temporaries are freed on return
   return cnt;
 }
 
@@ -885,7 +892,16 @@ int jk_mlp_forward(int nf, int count, const float *dX, const float *dParams, flo
 {
   if (nf != kMlpFeat) return -1;
   if (count < 0) return -2;
-  CK(mlp_forward(nf, count, dX, dParams, dY, (cudaStream_t)stream));
+  if (!count) return 0;
+  Guard g;
+  unsigned short *w = nullptr;
+  float *b = nullptr;
+  cudaStream_t s = (cudaStream_t)stream;
+  CK(g.alloc(&w, (kMlpHidden * nf + kMlpHidden * kMlpHidden + kMlpHidden) * sizeof(unsigned short)));
+  CK(g.alloc(&b, (2 * kMlpHidden + 1) * sizeof(float)));
+  CK(mlp_pack(nf, dParams, w, b, s));
+  CK(mlp_forward(nf, count, dX, w, b, dY, s));
+  CK(cudaStreamSynchronize(s));
   return 0;
 }
 

@@ -71,7 +71,7 @@ struct HypPar {
 
 // the scorer of a learned solve (device parameters)
 struct ScorerDev {
-  const unsigned short *w;  // bf16 weights W1 [64][nf], W2 [64][64], W3 [64]
+  const unsigned short *w;  // bf16 weights W1 [64][nf], W2 [64][64], W3 [64] (NULL: no network)
   const float *b;           // fp32 biases b1 [64], b2 [64], b3
   int nf;
 };
@@ -97,8 +97,8 @@ struct Workspace {
   double *offpart;   // per-block partial off-norms (learned solves)
   int *offcount;     // blocks done (the last one finishes the off-norm)
   int learned;       // rank the scanned hyperbolic pairs by `sc`
-  ScorerDev sc;      // sc.nf == 0: the Gram-guided ranking (no network)
-  double *gram;      // Gram-guided ranking: n_plus x n_minus off-diagonal column products
+  ScorerDev sc;      // sc.nf == 0: the Gram form alone (no network)
+  double *gram;      // scored steps: n_plus x n_minus products of the columns without their diagonal
   double *cn;        // ... and the columns' off-diagonal squared norms
   // ID_NCP = 3 (AW_NCP3): per record key and tie, the sorted order, every start's walk
   int id_ncp;
@@ -139,15 +139,15 @@ cudaError_t launch_batch(int variant, int grid, const BatchItem *items, int coun
 
 // the learned ranking (jk_scorer.cu)
 constexpr int kMlpHidden = 64;
-constexpr int kMlpFeat = 7;
+constexpr int kMlpFeat = 8;
 __host__ __device__ constexpr int mlp_params(int nf) { return kMlpHidden * nf + kMlpHidden + kMlpHidden * kMlpHidden + kMlpHidden + kMlpHidden + 1; }
 cudaError_t launch_learned_weights(Workspace &w, const double *A, cudaStream_t s);
 cudaError_t prepare_gram();
 constexpr int kOffBlocks = 296;  // fixed grid of the off-norm reduction (a fixed summation order)
 cudaError_t launch_offnorm(Workspace &w, const double *A, cudaStream_t s);
-cudaError_t mlp_features(int n, const double *A, const int *plus, const int *minus, int n_plus, int n_minus, int step, int nf,
-                         float *X, cudaStream_t s);
-cudaError_t mlp_forward(int nf, int count, const float *X, const float *params, float *Y, cudaStream_t s);
+cudaError_t mlp_features(int n, const double *A, const int *plus, const int *minus, int n_plus, int n_minus, int step,
+                         const State *st, double *G, double *cn, float *X, double *Wg, cudaStream_t s);
+cudaError_t mlp_forward(int nf, int count, const float *X, const unsigned short *w, const float *b, float *Y, cudaStream_t s);
 cudaError_t mlp_grad(int nf, int count, const float *X, const float *T, const float *params, float *grad, float *loss,
                      float *partial, cudaStream_t s);
 size_t mlp_grad_partial_floats(int nf, int count);

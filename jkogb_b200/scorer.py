@@ -1,11 +1,13 @@
 """The learned ranking: training data from the exact method's trajectories, training
 with the library's own forward/backward/Adam kernels, and the scored solve.
 
-The network (7 -> 64 -> 64 -> 1, ReLU, BF16 weights, FP32 biases and accumulation)
-predicts g(w) = sign(w) (log2|w| + 1100) / 1024 of a hyperbolic pair's exact weight w
-(DMAGF2H, src/D/dstep.F90:41-72) from the pair's 2x2 block; g is monotone, so ranking
-by the prediction ranks by the predicted weight.  Device memory here is torch's; all
-arithmetic runs in the library's kernels (jk_mlp_*).
+In a scored step the hyperbolic pairs that need the column scan are ranked by
+w_gram * 2^(clamp(y, -1, 1) / 8): w_gram is the off-norm reduction written through the
+Gram matrix of the columns without their diagonal (equal to the exact weight of DMAGF2H,
+src/D/dstep.F90:41-72, up to rounding) and y the output of a network 8 -> 64 -> 64 -> 1
+(ReLU, BF16 weights and inputs, FP32 biases and accumulation; tensor cores) trained to
+predict clamp(8 log2(w / w_gram), -1, 1) from the pair's Gram features.  Device memory here
+is torch's; all arithmetic runs in the library's kernels (jk_mlp_*).
 """
 from __future__ import annotations
 
@@ -15,7 +17,7 @@ import numpy as np
 
 from . import JkError, Handle, Opts, _opts, lib
 
-NF = 7
+NF = 8
 HIDDEN = 64
 
 
@@ -23,13 +25,15 @@ def nparams() -> int:
     return int(lib().jk_mlp_nparams(NF))
 
 
-def g_of(w):
-    """The training target of a weight: sign(w) (log2|w| + 1100) / 1024, 0 for w = 0."""
+def target_of(w, wg):
+    """The training target of a scanned pair: clamp(8 log2(w / w_gram), -1, 1), 0 where the
+    signs differ or either is zero."""
     w = np.asarray(w, np.float64)
-    a = np.abs(w)
-    with np.errstate(divide="ignore"):
-        lg = np.where(a > 0, np.log2(np.where(a > 0, a, 1.0)), 0.0)
-    return np.where(a > 0, np.sign(w) * (lg + 1100.0) / 1024.0, 0.0)
+    wg = np.asarray(wg, np.float64)
+    ok = (w != 0) & (wg != 0) & (np.sign(w) == np.sign(wg))
+    with np.errstate(divide="ignore", invalid="ignore"):
+        r = np.where(ok, 8.0 * np.log2(np.abs(np.where(ok, w, 1.0)) / np.abs(np.where(ok, wg, 1.0))), 0.0)
+    return np.clip(r, -1.0, 1.0)
 
 
 def init_params(seed=0) -> np.ndarray:
@@ -53,22 +57,26 @@ def _stream(torch, dev):
 
 def features(dA, J, step):
     """Features of every hyperbolic pair of the column-major device matrix dA (torch),
-    (+ index, - index) order; returns (X (count, 7) float32 on the device, plus, minus)."""
+    (+ index, - index) order; returns (X (count, 8) float32 on the device, w_gram (count)
+    float64 on the device, NaN for the pairs that need no scan, plus, minus)."""
     import torch
     n = dA.shape[0]
     Jc = np.ascontiguousarray(np.asarray(J, np.int32))
     plus = np.nonzero(Jc == 1)[0]
     minus = np.nonzero(Jc == -1)[0]
-    X = torch.empty((max(len(plus) * len(minus), 1), NF), dtype=torch.float32, device=dA.device)
-    cnt = lib().jk_mlp_features(n, _vp(dA), Jc.ctypes.data_as(C.POINTER(C.c_int)), int(step), _vp(X),
+    m = max(len(plus) * len(minus), 1)
+    X = torch.empty((m, NF), dtype=torch.float32, device=dA.device)
+    Wg = torch.empty(m, dtype=torch.float64, device=dA.device)
+    cnt = lib().jk_mlp_features(n, _vp(dA), Jc.ctypes.data_as(C.POINTER(C.c_int)), int(step), _vp(X), _vp(Wg),
                                 _stream(torch, dA.device))
     if cnt < 0:
         raise JkError(int(cnt), "features: ")
-    return X[:cnt], plus, minus
+    return X[:cnt], Wg[:cnt], plus, minus
 
 
 def forward(X, params):
-    """The network on device features X (count, 7); params a device float32 tensor."""
+    """The network (the inference arithmetic) on device features X (count, 8); params a device
+    float32 tensor of master parameters."""
     import torch
     Y = torch.empty(X.shape[0], dtype=torch.float32, device=X.device)
     rc = lib().jk_mlp_forward(NF, X.shape[0], _vp(X.contiguous()), _vp(params), _vp(Y), _stream(torch, X.device))
@@ -93,9 +101,9 @@ def grad(X, T, params):
 
 
 def training_data(mats, Js, every=4, max_pairs=4096, seed=0):
-    """Features and targets along the exact method's trajectories: every `every`-th
-    step of each solve, up to max_pairs finite hyperbolic pairs per sampled step.
-    Returns (X, T) as device tensors."""
+    """Features and targets along the exact method's trajectories: every `every`-th step of
+    each solve, up to max_pairs scanned hyperbolic pairs with a finite weight per sampled
+    step.  Returns (X, T) as device tensors."""
     import torch
     import jkogb_b200 as jk
     r = np.random.Generator(np.random.PCG64(seed))
@@ -111,17 +119,17 @@ def training_data(mats, Js, every=4, max_pairs=4096, seed=0):
         h = Handle(n, J)
         step = 0
         while True:
-            X, plus, minus = features(A, J, step)
+            X, Wg, plus, minus = features(A, J, step)
             h.weights(A.data_ptr(), W.data_ptr(), torch.cuda.current_stream(dev).cuda_stream)
             w = W[torch.from_numpy(plus).to(dev)][:, torch.from_numpy(minus).to(dev)].reshape(-1)
-            ok = torch.isfinite(w)
+            ok = torch.isfinite(w) & torch.isfinite(Wg)
             idx = torch.nonzero(ok).reshape(-1)
-            if idx.numel() == 0:
-                break
             if idx.numel() > max_pairs:
                 idx = idx[torch.from_numpy(r.choice(idx.numel(), max_pairs, replace=False)).to(dev)]
-            xs.append(X[idx].clone())
-            ts.append(torch.from_numpy(g_of(w[idx].cpu().numpy()).astype(np.float32)).to(dev))
+            if idx.numel():
+                xs.append(X[idx].clone())
+                t = target_of(w[idx].cpu().numpy(), Wg[idx].cpu().numpy())
+                ts.append(torch.from_numpy(t.astype(np.float32)).to(dev))
             info = jk.step_loop_dev(A, U, Z, s, J, max_steps=every)
             if info != -24:
                 break
@@ -204,5 +212,5 @@ class Scorer:
             pass
 
 
-__all__ = ["NF", "nparams", "g_of", "init_params", "features", "forward", "grad", "training_data", "train", "Scorer",
-           "Opts"]
+__all__ = ["NF", "nparams", "target_of", "init_params", "features", "forward", "grad", "training_data", "train",
+           "Scorer", "Opts"]

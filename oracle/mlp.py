@@ -2,15 +2,16 @@
 features and its training step, the checker of the library's jk_mlp_* kernels.
 
 The network has no counterpart in the reference.  Layout of the FP32 parameter vector:
-W1 [64][7] row-major, b1 [64], W2 [64][64], b2 [64], W3 [64], b3.  Weights enter the
-arithmetic rounded to BF16 (round to nearest even), biases as they are; everything here
-is computed in float64.
+W1 [64][8] row-major, b1 [64], W2 [64][64], b2 [64], W3 [64], b3.  Inputs, weights and the
+first layer's activations enter the arithmetic rounded to BF16 (round to nearest even),
+biases as they are; everything else here is computed in float64.  The features are the
+Gram quantities of a scanned hyperbolic pair (see features()).
 """
 from __future__ import annotations
 
 import numpy as np
 
-NF = 7
+NF = 8
 H = 64
 
 
@@ -33,35 +34,65 @@ def unpack(P):
     return W1, b1, W2, b2, W3, b3
 
 
+def _lg64(x):
+    a = abs(float(x))
+    return np.float32((np.log2(a) if a > 0 else -1074.0) / 64.0)
+
+
 def features(A, J, step):
-    """Features of every hyperbolic pair, (+ index, - index) order (see jk_mlp_features)."""
+    """Features and w_gram of every hyperbolic pair, (+ index, - index) order (see
+    jk_mlp_features): for a pair (p, q) that needs the column scan, with x = A(:,p), y = A(:,q)
+    without rows p, q and Z2 the pair's 2x2 right transformation,
+      w_gram = d0 + nx (1 - Z11^2 - Z12^2) + ny (1 - Z21^2 - Z22^2) - 2 (Z11 Z21 + Z12 Z22) g,
+    nx = x.x, ny = y.y, g = x.y, d0 the two leading terms of ABODNDF2; the features are the
+    BF16 roundings of log2/64 of |w_gram|, nx, ny, |g|, |d0|, |Z12| + |Z21|, sign(w_gram) and
+    min(S / (10 N), 4).  Other pairs: zero features and w_gram NaN.  Returns (X, w_gram)."""
+    import oracle
     A = np.asarray(A, np.float64)
     n = A.shape[0]
     J = np.asarray(J)
     plus = np.nonzero(J == 1)[0]
     minus = np.nonzero(J == -1)[0]
-    X = np.zeros((len(plus) * len(minus), NF), np.float32)
-
-    def lg(x):
-        a = abs(x)
-        return np.float32((np.log2(a) if a > 0 else -1074.0) / 64.0)
-
-    k = 0
+    X = np.zeros((len(plus) * len(minus), NF), np.float64)
+    Wg = np.full(len(plus) * len(minus), np.nan)
+    A0 = A.copy()
+    np.fill_diagonal(A0, 0.0)
+    k = -1
     for a in plus:
         for b in minus:
-            p, q = (a, b) if a < b else (b, a)
-            X[k] = [lg(A[p, q]), lg(A[q, p]), lg(A[p, p]), lg(A[q, q]), float(J[p]), float(J[q]),
-                    min(np.float32(step) / np.float32(10.0 * n), np.float32(4.0))]
             k += 1
-    return X
+            p, q = (a, b) if a < b else (b, a)
+            jp = 1 if a < b else -1
+            app, aqp, apq, aqq = A[p, p], A[q, p], A[p, q], A[q, q]
+            if not (aqp != 0 or apq != 0 or np.signbit(app) or np.signbit(aqq)):
+                continue
+            A2, U2, Z2, info = oracle.hsvd2(np.array([[app, apq], [aqp, aqq]]), [jp, -jp])
+            if info < 0 or not (info & 1) or not (info & 4):
+                continue
+            a1 = A2[1, 0] if info & 8 else 0.0
+            a2 = A2[0, 1] if info & 8 else 0.0
+            d = (aqp - a1) * (aqp + a1) + (apq - a2) * (apq + a2)
+            z11, z21, z12, z22 = Z2[0, 0], Z2[1, 0], Z2[0, 1], Z2[1, 1]
+            x, y = A0[:, p].copy(), A0[:, q].copy()
+            x[q] = 0.0
+            y[p] = 0.0
+            nx, ny, g = float(x @ x), float(y @ y), float(x @ y)
+            c1 = (1.0 - z11) * (1.0 + z11) - z12 * z12
+            c2 = (1.0 - z22) * (1.0 + z22) - z21 * z21
+            c3 = z11 * z21 + z12 * z22
+            w = d + (nx * c1 + ny * c2 - 2.0 * c3 * g)
+            Wg[k] = w
+            X[k] = bf16([_lg64(w), -1.0 if w < 0 else 1.0, _lg64(nx), _lg64(ny), _lg64(g), _lg64(d),
+                         _lg64(abs(z12) + abs(z21)), min(np.float32(step) / np.float32(10.0 * n), np.float32(4.0))])
+    return X.astype(np.float32), Wg
 
 
 def forward(X, P):
     W1, b1, W2, b2, W3, b3 = unpack(P)
     W1, W2, W3 = bf16(W1), bf16(W2), bf16(W3)
-    X = np.asarray(X, np.float64)
+    X = bf16(np.asarray(X, np.float32))
     z1 = X @ W1.T + b1
-    h1 = np.maximum(z1, 0.0)
+    h1 = bf16(np.maximum(z1, 0.0).astype(np.float32))
     z2 = h1 @ W2.T + b2
     h2 = np.maximum(z2, 0.0)
     return h2 @ W3 + float(b3), (X, z1, h1, z2, h2)
@@ -69,7 +100,7 @@ def forward(X, P):
 
 def loss_grad(X, T, P):
     """Mean squared error and its gradient with respect to the parameter vector
-    (straight through the BF16 rounding of the weights)."""
+    (straight through the BF16 rounding of the weights and of the first layer's outputs)."""
     W1, b1, W2, b2, W3, b3 = unpack(P)
     y, (X, z1, h1, z2, h2) = forward(X, P)
     T = np.asarray(T, np.float64)
