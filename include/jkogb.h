@@ -180,6 +180,13 @@ int jk_batch_run(jk_batch *b, double *dA, double *dU, double *dZ, double *dsigma
  * each), keeps the fastest for later runs and returns its thread count.  dA is left
  * unchanged; dU, dZ, dsigma, dinfo are overwritten (scratch). */
 int jk_batch_tune(jk_batch *b, const double *dA, double *dU, double *dZ, double *dsigma, int *dinfo, void *stream);
+/* Rank the batch's scanned hyperbolic pairs by the Gram form of their weights (a scorer
+ * made by jk_scorer_create with nf = 0; see the learned ranking below), with the same
+ * fallback to the exact weights; sc NULL: the exact weights (the default).  Later runs and
+ * tunes use it.  Returns 0, -1 (b NULL) or -2 (a scorer with a network: the batched kernel
+ * has no room for one in shared memory). */
+typedef struct jk_scorer jk_scorer;
+int jk_batch_set_scorer(jk_batch *b, const jk_scorer *sc);
 /* The same with host buffers (copies in and out, synchronous).  Returns 0 or an error. */
 int jk_dstep_loop_batched(int count, const int *n, const int *n_2, double *A, double *U, double *Z, const int *J,
                           double *sigma, int *info, const jk_opts *opts);
@@ -207,7 +214,6 @@ int jk_dstep_loop_batched(int count, const int *n, const int *n_2, double *A, do
  * b2 [64], W3 [64], b3: jk_mlp_nparams(8) = 4801 floats.  jk_scorer_create with nf = 0 and
  * params NULL ranks by w_gram alone (no network). */
 #define JK_MLP_FEATURES 8
-typedef struct jk_scorer jk_scorer;
 int jk_mlp_nparams(int nf);
 jk_scorer *jk_scorer_create(int nf, const float *params, int stall_k, int *info);
 void jk_scorer_destroy(jk_scorer *sc);

@@ -34,7 +34,7 @@ SYMBOLS = ("jk_dstep_loop", "jk_zstep_loop", "jk_dstep_loop_dev", "jk_zstep_loop
            "jk_solver_finish", "jk_dhsvd2_batch",
            "jk_zhsvd2_batch", "jk_dweights", "jk_zweights", "jk_select", "jk_handle_create", "jk_handle_destroy",
            "jk_handle_weights", "jk_dweights_noalloc", "jk_batch_create", "jk_batch_destroy",
-           "jk_batch_run", "jk_batch_tune", "jk_dstep_loop_batched", "jk_mlp_nparams", "jk_scorer_create",
+           "jk_batch_run", "jk_batch_tune", "jk_batch_set_scorer", "jk_dstep_loop_batched", "jk_mlp_nparams", "jk_scorer_create",
            "jk_scorer_destroy", "jk_dstep_loop_dev_scored", "jk_mlp_features", "jk_mlp_forward", "jk_mlp_grad_workspace",
            "jk_mlp_grad", "jk_mlp_adam", "jk_last_launch_count", "jk_fp64_peak", "jk_max_order", "jk_strerror")
 
@@ -119,6 +119,8 @@ def lib():
         L.jk_batch_run.argtypes = [C.c_void_p, vp, vp, vp, vp, vp, vp]
         L.jk_batch_tune.restype = C.c_int
         L.jk_batch_tune.argtypes = [C.c_void_p, vp, vp, vp, vp, vp, vp]
+        L.jk_batch_set_scorer.restype = C.c_int
+        L.jk_batch_set_scorer.argtypes = [C.c_void_p, C.c_void_p]
         L.jk_mlp_nparams.restype = C.c_int
         L.jk_mlp_nparams.argtypes = [C.c_int]
         L.jk_scorer_create.restype = C.c_void_p
@@ -449,6 +451,13 @@ class Batch:
         rc = lib().jk_batch_run(self._b, dA, dU, dZ, dsigma, dinfo, C.c_void_p(stream))
         if rc < 0:
             raise JkError(rc, "batch run: ")
+
+    def set_scorer(self, scorer):
+        """Rank by the Gram form of the scanned weights (a scorer.Scorer made without a
+        network), or by the exact weights (None)."""
+        rc = lib().jk_batch_set_scorer(self._b, scorer._s if scorer is not None else None)
+        if rc < 0:
+            raise JkError(rc, "batch scorer: ")
 
     def tune(self, dA, dU, dZ, dsigma, dinfo, stream=0):
         """Choose the block shape on this batch; returns the chosen threads per block."""

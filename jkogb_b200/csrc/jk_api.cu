@@ -616,7 +616,8 @@ struct jk_batch {
   int *counter = nullptr, *J = nullptr;
   cudaGraphExec_t exec = nullptr;
   const void *key[6] = {};  // the buffers and stream the graph was captured with
-  int key_variant = -1;
+  int key_variant = -1, key_scored = -1;
+  int scored = 0, stall_k = 8;  // the Gram-form ranking (jk_batch_set_scorer)
   ~jk_batch()
   {
     if (exec) cudaGraphExecDestroy(exec);
@@ -702,7 +703,7 @@ int jk_batch_run(jk_batch *b, double *dA, double *dU, double *dZ, double *dsigma
   if (!b || !dA || !dU || !dZ || !dsigma || !dinfo) return -1;
   cudaStream_t s = (cudaStream_t)stream;
   const void *key[6] = { dA, dU, dZ, dsigma, dinfo, stream };
-  bool same = (b->exec != nullptr) && (b->key_variant == b->variant);
+  bool same = (b->exec != nullptr) && (b->key_variant == b->variant) && (b->key_scored == b->scored);
   for (int k = 0; k < 6; ++k) same = same && (key[k] == b->key[k]);
   if (!same) {
     if (b->exec) { cudaGraphExecDestroy(b->exec); b->exec = nullptr; }
@@ -711,7 +712,7 @@ int jk_batch_run(jk_batch *b, double *dA, double *dU, double *dZ, double *dsigma
     cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
     if (e == cudaSuccess) {
       const cudaError_t e1 = launch_batch(b->variant, b->grid, b->items, b->count, b->counter, dA, dU, dZ, b->J, dsigma,
-                                          dinfo, b->nm, b->cap, s);
+                                          dinfo, b->nm, b->cap, b->scored, b->stall_k, s);
       const cudaError_t e2 = cudaStreamEndCapture(s, &graph);
       e = (e1 != cudaSuccess) ? e1 : e2;
     }
@@ -722,14 +723,24 @@ int jk_batch_run(jk_batch *b, double *dA, double *dU, double *dZ, double *dsigma
       b->exec = nullptr;
       g_launches = 1;
       CK(launch_batch(b->variant, b->grid, b->items, b->count, b->counter, dA, dU, dZ, b->J, dsigma, dinfo, b->nm,
-                      b->cap, s));
+                      b->cap, b->scored, b->stall_k, s));
       return 0;
     }
     for (int k = 0; k < 6; ++k) b->key[k] = key[k];
     b->key_variant = b->variant;
+    b->key_scored = b->scored;
   }
   g_launches = 1;
   CK(cudaGraphLaunch(b->exec, s));
+  return 0;
+}
+
+int jk_batch_set_scorer(jk_batch *b, const jk_scorer *sc)
+{
+  if (!b) return -1;
+  if (sc && sc->nf != 0) return -2;  // the batched kernel ranks by the Gram form only
+  b->scored = sc ? 1 : 0;
+  b->stall_k = sc ? sc->stall_k : 8;
   return 0;
 }
 
@@ -756,7 +767,8 @@ int jk_batch_tune(jk_batch *b, const double *dA, double *dU, double *dZ, double 
     err = cudaMemcpyAsync(scratch, dA, b->total * sizeof(double), cudaMemcpyDeviceToDevice, s);
     if (err == cudaSuccess) err = cudaEventRecord(e0, s);
     if (err == cudaSuccess)
-      err = launch_batch(v, grid, b->items, sub, b->counter, scratch, dU, dZ, b->J, dsigma, dinfo, b->nm, cap_t, s);
+      err = launch_batch(v, grid, b->items, sub, b->counter, scratch, dU, dZ, b->J, dsigma, dinfo, b->nm, cap_t, b->scored,
+                         b->stall_k, s);
     if (err == cudaSuccess) err = cudaEventRecord(e1, s);
     if (err == cudaSuccess) err = cudaEventSynchronize(e1);
     float ms = 0.0f;

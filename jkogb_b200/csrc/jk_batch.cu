@@ -44,7 +44,7 @@ __host__ __device__ __forceinline__ size_t align16(size_t x) { return (x + 15) &
 
 // shared-memory layout for the largest order nm of the batch
 struct BLayout {
-  size_t a, w, piv, pairs, rank, pos, vlist, jv, best, ms, total;
+  size_t a, w, piv, pairs, rank, pos, vlist, jv, best, ms, cn, total;
   __host__ __device__ explicit BLayout(int nm)
   {
     const int h = nm / 2 + 1;
@@ -58,7 +58,8 @@ struct BLayout {
     jv = align16(vlist + (size_t)nm * sizeof(int));
     best = align16(jv + (size_t)nm * sizeof(int));
     ms = align16(best + (size_t)nm * sizeof(int));
-    total = ms;
+    cn = align16(ms);
+    total = cn + (size_t)nm * sizeof(double);
   }
 };
 
@@ -98,10 +99,17 @@ __device__ __forceinline__ void scan_pair(const double *xs, const double *ys, in
   }
 }
 
+// scored: rank the scanned hyperbolic pairs by the Gram form of their weights (squared
+// column norms and the column products without rows p, q; one fma per row instead of the
+// scan's ten operations), with the fallback rules of the single-matrix scored loop: after
+// stall_k steps without a new minimum of the off-norm the next step ranks exactly, a
+// scored step without an effective pivot is followed by an exact step (only an exact
+// step ends the loop), and once the off-norm exceeds 16 times its minimum the rest of
+// the solve ranks exactly
 template <int THREADS>
 __device__ void solve_one(const BatchItem &it, double *__restrict__ gA, double *__restrict__ gU, double *__restrict__ gZ,
                           const int *__restrict__ gJ, double *__restrict__ gsigma, int *__restrict__ ginfo, int nm,
-                          long long cap, unsigned char *smem)
+                          long long cap, int scored, int stall_k, unsigned char *smem)
 {
   const BLayout L(nm);
   double *As = (double *)(smem + L.a);
@@ -113,7 +121,10 @@ __device__ void solve_one(const BatchItem &it, double *__restrict__ gA, double *
   int *vl = (int *)(smem + L.vlist);     // shared-memory column -> vertex (+ columns, then - columns)
   int *Jv = (int *)(smem + L.jv);
   int *suitor = (int *)(smem + L.best);  // per vertex: its current suitor (-1: none)
+  double *cn = (double *)(smem + L.cn);  // scored steps: squared off-diagonal column norms
   __shared__ int s_np, s_cnt, s_nl, s_err;
+  __shared__ int s_learned, s_lstep, s_retry, s_stall;  // the scored ranking's state
+  __shared__ double s_best, s_red[THREADS / 32];
 
   const int tid = threadIdx.x, n = it.n, lda = n + 1, v_ = tid;
   double *A = gA + it.off, *U = gU + it.off, *Z = gZ + it.off;
@@ -155,8 +166,27 @@ __device__ void solve_one(const BatchItem &it, double *__restrict__ gA, double *
   const int np = s_np, nmn = n - np;
   const int nn = n * (n - 1) / 2;
   int steps = 0, info = 0;
+  if (tid == 0) {
+    s_learned = scored;
+    s_lstep = scored;
+    s_retry = 0;
+    s_stall = 0;
+    s_best = __longlong_as_double(0x7FF0000000000000LL);  // +inf
+  }
+  __syncthreads();
 
   for (;;) {
+    const bool lstep = s_lstep;  // this step ranks by the Gram form
+    if (lstep) {
+      for (int v = tid; v < n; v += THREADS) {
+        const double *c = As + pos[v] * lda;
+        double a = 0.0;
+        for (int i = 0; i < n; ++i)
+          if (i != v) a = fma(c[i], c[i], a);
+        cn[v] = a;
+      }
+      __syncthreads();
+    }
     // ---- weights of the trigonometric pairs (DMAGF2T)
     for (int k = tid; k < nn; k += THREADS) {
       int q = (int)((1.0 + sqrt(8.0 * k + 1.0)) * 0.5);
@@ -177,7 +207,29 @@ __device__ void solve_one(const BatchItem &it, double *__restrict__ gA, double *
     // with up to 384 threads two pairs per thread, their fma chains interleaved (the
     // 512-thread shape has no registers to spare for it)
     const int nh = np * nmn;
-    if constexpr (THREADS > 384) {
+    if (lstep) {
+      // the Gram form: per pair the product of its columns without rows p, q
+      for (int k = tid; k < nh; k += THREADS) {
+        const int ci = k / nmn, cj = np + k % nmn;  // shared-memory columns
+        const int a = vl[ci], b = vl[cj];
+        const bool a_is_p = a < b;
+        const int p = a_is_p ? a : b, q = a_is_p ? b : a;
+        const double *xs = As + (a_is_p ? ci : cj) * lda, *ys = As + (a_is_p ? cj : ci) * lda;
+        double w, d = 0.0, Z2[4];
+        if (hyp_setup_z(xs[p], xs[q], ys[p], ys[q], a_is_p ? 1 : -1, w, d, Z2)) {
+          double g = 0.0;
+#pragma unroll 4
+          for (int i = 0; i < n; ++i) {
+            const double e = fma(xs[i], ys[i], g);
+            g = (i != p && i != q) ? e : g;
+          }
+          w = gram_weight(d, Z2, cn[p] - xs[q] * xs[q], cn[q] - ys[p] * ys[p], g);
+        }
+        if (w < -JK_HUGE) w = nan_w();
+        Ws[tri(p, q)] = w;
+      }
+    }
+    else if constexpr (THREADS > 384) {
       for (int k = tid; k < nh; k += THREADS) {
         const int ci = k / nmn, cj = np + k % nmn;  // shared-memory columns
         const int a = vl[ci], b = vl[cj];
@@ -402,10 +454,55 @@ __device__ void solve_one(const BatchItem &it, double *__restrict__ gA, double *
       }
     }
     __syncthreads();
-    // ---- the loop test
     const int nl = s_nl;
+    if (s_learned && err == 0) {
+      // ---- the scored ranking: the off-norm after the step (fixed summation order) and
+      // the choice of the next step's ranking
+      double acc = 0.0;
+      for (int k = tid; k < n * n; k += THREADS) {
+        const int i = k % n, j = k / n;
+        if (i != j) {
+          const double x = As[pos[j] * lda + i];
+          acc = fma(x, x, acc);
+        }
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xFFFFFFFFu, acc, o);
+      if ((tid & 31) == 0) s_red[tid >> 5] = acc;
+      __syncthreads();
+      if (tid == 0) {
+        double off = 0.0;
+        for (int w = 0; w < THREADS / 32; ++w) off += s_red[w];
+        if (s_lstep && ((sl < nl) ? sl : nl) <= 0) {
+          s_retry = 1;  // no effective pivot among the scored choices: an exact step decides
+          s_lstep = 0;
+          s_stall = 0;
+        }
+        else if (off > 16.0 * s_best) {
+          s_learned = 0;  // the scored choices let the off-norm grow: the rest ranks exactly
+          s_lstep = 0;
+        }
+        else {
+          if (off < s_best) { s_best = off; s_stall = 0; }
+          else s_stall += 1;
+          if (s_stall >= stall_k) { s_lstep = 0; s_stall = 0; }
+          else s_lstep = 1;
+        }
+      }
+      __syncthreads();
+    }
+    // ---- the loop test
     if (err < 0) { info = err; break; }
-    if (((sl < nl) ? sl : nl) <= 0) { info = steps; break; }
+    if (((sl < nl) ? sl : nl) <= 0) {
+      if (s_retry) {
+        __syncthreads();
+        if (tid == 0) s_retry = 0;
+        __syncthreads();
+        continue;
+      }
+      info = steps;
+      break;
+    }
     ++steps;
     if (steps >= cap) { info = kInfoMaxSteps; break; }
     __syncthreads();
@@ -438,7 +535,7 @@ __device__ void solve_one(const BatchItem &it, double *__restrict__ gA, double *
 template <int THREADS>
 __global__ void __launch_bounds__(THREADS, 1)
 k_batch(const BatchItem *__restrict__ items, int count, int *counter, double *A, double *U, double *Z, const int *J,
-        double *sigma, int *info, int nm, long long cap)
+        double *sigma, int *info, int nm, long long cap, int scored, int stall_k)
 {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ int s_m;
@@ -448,7 +545,7 @@ k_batch(const BatchItem *__restrict__ items, int count, int *counter, double *A,
     const int m = s_m;
     __syncthreads();
     if (m >= count) break;
-    solve_one<THREADS>(items[m], A, U, Z, J, sigma, info, nm, cap, smem_raw);
+    solve_one<THREADS>(items[m], A, U, Z, J, sigma, info, nm, cap, scored, stall_k, smem_raw);
   }
 }
 
@@ -482,15 +579,16 @@ int batch_blocks_per_sm(int variant, int nm)
 }
 
 cudaError_t launch_batch(int variant, int grid, const BatchItem *items, int count, int *counter, double *A, double *U,
-                         double *Z, const int *J, double *sigma, int *info, int nm, long long cap, cudaStream_t s)
+                         double *Z, const int *J, double *sigma, int *info, int nm, long long cap, int scored, int stall_k,
+                         cudaStream_t s)
 {
   const size_t sm = batch_smem(nm);
   cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(int), s);
   if (e != cudaSuccess) return e;
   switch (variant) {
-  case 0: k_batch<256><<<grid, 256, sm, s>>>(items, count, counter, A, U, Z, J, sigma, info, nm, cap); break;
-  case 1: k_batch<384><<<grid, 384, sm, s>>>(items, count, counter, A, U, Z, J, sigma, info, nm, cap); break;
-  default: k_batch<512><<<grid, 512, sm, s>>>(items, count, counter, A, U, Z, J, sigma, info, nm, cap); break;
+  case 0: k_batch<256><<<grid, 256, sm, s>>>(items, count, counter, A, U, Z, J, sigma, info, nm, cap, scored, stall_k); break;
+  case 1: k_batch<384><<<grid, 384, sm, s>>>(items, count, counter, A, U, Z, J, sigma, info, nm, cap, scored, stall_k); break;
+  default: k_batch<512><<<grid, 512, sm, s>>>(items, count, counter, A, U, Z, J, sigma, info, nm, cap, scored, stall_k); break;
   }
   return cudaGetLastError();
 }

@@ -112,4 +112,37 @@ __device__ __forceinline__ bool hyp_setup(double app, double aqp, double apq, do
   return true;
 }
 
+// hyp_setup with the pair's 2x2 right transformation Z2 (column-major) instead of its AB
+// coefficients, for the Gram form of the scanned weight
+__device__ __forceinline__ bool hyp_setup_z(double app, double aqp, double apq, double aqq, int jp, double &w, double &d,
+                                            double Z2[4])
+{
+  w = nan_w();
+  if (!may_transform(app, aqp, apq, aqq)) return false;
+  double A2[4] = { app, aqp, apq, aqq }, U2[4];
+  int info = 0;
+  dhsvd2(A2, jp, -jp, U2, Z2, JK_TH1FIX, info);
+  if (info < 0) return false;
+  if (!(info & 1)) { w = 0.0; return false; }
+  if (!(info & 4)) { w = dasum2(aqp, apq); return false; }
+  const double a1 = (info & 8) ? A2[M21] : 0.0, a2 = (info & 8) ? A2[M12] : 0.0;
+  d = 0.0;
+  d = fma(__dsub_rn(aqp, a1), __dadd_rn(aqp, a1), d);
+  d = fma(__dsub_rn(apq, a2), __dadd_rn(apq, a2), d);
+  return true;
+}
+
+// the Gram form of a scanned hyperbolic weight: d + nx (1 - Z11^2 - Z12^2) +
+// ny (1 - Z21^2 - Z22^2) - 2 (Z11 Z21 + Z12 Z22) g, with nx, ny, g the squared norms and the
+// product of the pair's columns without rows p, q (the terms 1 - Z11^2 - Z12^2 and
+// 1 - Z21^2 - Z22^2 formed without cancellation at Z11, Z22 near +-1)
+__device__ __forceinline__ double gram_weight(double d, const double Z2[4], double nx, double ny, double g)
+{
+  const double z11 = Z2[M11], z21 = Z2[M21], z12 = Z2[M12], z22 = Z2[M22];
+  const double c1 = (1.0 - z11) * (1.0 + z11) - z12 * z12;
+  const double c2 = (1.0 - z22) * (1.0 + z22) - z21 * z21;
+  const double c3 = z11 * z21 + z12 * z22;
+  return d + (nx * c1 + ny * c2 - 2.0 * c3 * g);
+}
+
 }  // namespace jk

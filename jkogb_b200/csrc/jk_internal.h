@@ -135,7 +135,8 @@ size_t batch_smem(int nm);
 cudaError_t batch_prepare(int nm);
 int batch_blocks_per_sm(int variant, int nm);
 cudaError_t launch_batch(int variant, int grid, const BatchItem *items, int count, int *counter, double *A, double *U,
-                         double *Z, const int *J, double *sigma, int *info, int nm, long long cap, cudaStream_t s);
+                         double *Z, const int *J, double *sigma, int *info, int nm, long long cap, int scored, int stall_k,
+                         cudaStream_t s);
 
 // the learned ranking (jk_scorer.cu)
 constexpr int kMlpHidden = 64;
