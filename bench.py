@@ -416,6 +416,28 @@ def run_ours(args, wl):
     solve_ms = max_over_ranks(dev_ms, dev)
     sig_dev = s.cpu().numpy()
     solver.close()
+    sig_ref = _sigma_reference(args.workload)
+    sig_err = _sigma_err(sig_dev, sig_ref, J)
+
+    # the learned form on the same input: the scored ranking (the trained network's
+    # correction of the Gram form of the scanned weights), one device solve
+    learned = None
+    if not cplx and os.path.exists(scorer_mod().PARAMS):
+        sc = scorer_mod().Scorer(scorer_mod().load_params(), stall_k=8)
+        A.copy_(Y0)
+        barrier()
+        l0, l1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        l0.record(stream)
+        linfo, lexact = sc.step_loop_dev(A, U, Z, s, J, n_2=n_2, stream=stream)
+        l1.record(stream)
+        barrier()
+        l_ms = max_over_ranks(l0.elapsed_time(l1), dev)
+        sc.close()
+        learned = {"ranking": "trained network correcting the Gram form of the scanned hyperbolic weights",
+                   "solves_per_s": ws * 1e3 / l_ms, "solve_ms": l_ms, "solver_steps": linfo,
+                   "exact_steps": lexact, "ms_per_solver_step": l_ms / max(linfo, 1),
+                   "sigma_rel_err": _sigma_err(s.cpu().numpy(), sig_ref, J),
+                   "speedup_vs_plain": solve_ms / l_ms}
 
     # end to end: one solve through the host-pointer C ABI (H2D of Y, D2H of A, U, Z, SIGMA inside)
     Yh = np.asfortranarray(Y)
@@ -463,6 +485,10 @@ def run_ours(args, wl):
                    "step": "one benchmark step = 1/K of one full solve (the solve cut at solver-step "
                            f"boundaries into K = {args.steps} slices of {per_slice} solver steps, the last to the end)",
                    "solver_steps_to_converge": info, "ms_per_solver_step": solve_ms / max(info, 1),
+                   "sigma_rel_err": sig_err,
+                   "sigma_reference": "extended-precision one-sided hyperbolic Jacobi of the same input "
+                                      "(tests/golden/sigma_ref.npz), max relative error per J class",
+                   "learned": learned,
                    "slice_ms": [round(x, 3) for x in slice_ms],
                    "warmup": f"{args.warmup} prefix solves of 32 solver steps",
                    "parallelism": f"replicas{ws}", "l2": "working set > L2 (A, U, Z, W: 4 x 32 MB + ranking lists)"},
@@ -485,6 +511,33 @@ def run_ours(args, wl):
                                "sample": f"{nsteps} solver steps of the same solve on all host cores "
                                          f"({sec:.3f} s/step) x {steps_conv} steps to converge (extrapolated)"}
     print(json.dumps(out))
+
+
+def scorer_mod():
+    from jkogb_b200 import scorer
+    return scorer
+
+
+def _sigma_reference(workload):
+    """The workload's hyperbolic singular values from the accuracy oracle's fixture."""
+    try:
+        return np.load(os.path.join(ROOT, "tests", "golden", "sigma_ref.npz"))[workload]
+    except Exception:
+        return None
+
+
+def _sigma_err(sig, ref, J):
+    """Max relative error of sig against ref within each J sign class (both sorted)."""
+    if ref is None:
+        return None
+    J = np.asarray(J)
+    e = 0.0
+    for c in (1, -1):
+        m = J == c
+        if m.any():
+            a, b = np.sort(np.asarray(sig)[m]), np.sort(np.asarray(ref)[m])
+            e = max(e, float(np.max(np.abs(a - b) / np.abs(b))))
+    return e
 
 
 def _recorded_traffic(workload):

@@ -12,6 +12,7 @@ is torch's; all arithmetic runs in the library's kernels (jk_mlp_*).
 from __future__ import annotations
 
 import ctypes as C
+import os
 
 import numpy as np
 
@@ -212,5 +213,54 @@ class Scorer:
             pass
 
 
+PARAMS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "scorer_params.npy")
+
+
+def training_set(count=64, nmin=64, nmax=512, seed=0):
+    """`count` seeded training matrices with orders in [nmin, nmax]: half graded (column
+    scales log-uniform down to 1e-2 .. 1e-8), half iid Gaussian, J of random signs."""
+    from . import gen
+    r = np.random.Generator(np.random.PCG64(seed))
+    out = []
+    for k in range(count):
+        n = int(r.integers(nmin // 2, nmax // 2 + 1)) * 2
+        if k % 2 == 0:
+            Y, J = gen.graded(n, float(10.0 ** -r.integers(2, 9)), seed=int(r.integers(1 << 30)))
+        else:
+            Y, J = gen.gaussian(n, seed=int(r.integers(1 << 30)), n_plus=int(r.integers(n // 5, 4 * n // 5 + 1)))
+        out.append((Y, J))
+    return out
+
+
+def load_params(path=PARAMS):
+    """The committed trained parameters (see main())."""
+    return np.load(path).astype(np.float32)
+
+
+def main(argv=None):
+    """Train the network on the exact method's trajectories of training_set() and save the
+    FP32 master parameters:  python -m jkogb_b200.scorer [--solves C] [--iters I] [--out F]"""
+    import argparse
+    ap = argparse.ArgumentParser(prog="python -m jkogb_b200.scorer")
+    ap.add_argument("--solves", type=int, default=64)
+    ap.add_argument("--nmin", type=int, default=64)
+    ap.add_argument("--nmax", type=int, default=512)
+    ap.add_argument("--every", type=int, default=16)
+    ap.add_argument("--pairs", type=int, default=512)
+    ap.add_argument("--iters", type=int, default=3000)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--out", default=PARAMS)
+    a = ap.parse_args(argv)
+    mats = training_set(a.solves, a.nmin, a.nmax, a.seed)
+    X, T = training_data([m for m, _ in mats], [j for _, j in mats], every=a.every, max_pairs=a.pairs, seed=a.seed)
+    P, hist = train(X, T, iters=a.iters, seed=a.seed, log=lambda it, l: print(f"iter {it} loss {l:.3e}", flush=True))
+    np.save(a.out, P)
+    print(f"{X.shape[0]} samples from {len(mats)} solves; loss {hist[0][1]:.3e} -> {hist[-1][1]:.3e}; saved {a.out}")
+
+
 __all__ = ["NF", "nparams", "target_of", "init_params", "features", "forward", "grad", "training_data", "train",
-           "Scorer", "Opts"]
+           "Scorer", "Opts", "training_set", "load_params", "PARAMS", "main"]
+
+
+if __name__ == "__main__":
+    main()
