@@ -256,13 +256,21 @@ __device__ __forceinline__ bool hyp_pair_setup(const double *__restrict__ A, int
 #define SCAN_ROWS 64
 #define SCAN_RS (SCAN_ROWS + 2)
 
-// K pairs per thread (slots t, t + 256, ...); FAST: no row of this chunk is a p or q
-template <int K, bool FAST>
+// rows of a chunk unrolled together in the scan (a tuning knob; 2 unless set at build time)
+#ifndef JK_SCAN_UNROLL
+#define JK_SCAN_UNROLL 2
+#endif
+constexpr int kScanUnroll = JK_SCAN_UNROLL;
+
+// K pairs per thread (slots t, t + 256, ...); FAST: no row of this chunk is a p or q;
+// FULL: the chunk has all SCAN_ROWS rows (a compile-time trip count, no bound test)
+template <int K, bool FAST, bool FULL>
 __device__ __forceinline__ void scan_chunk(const double *const *xs, const double *const *ys, const int *pl, const int *ql,
                                            const int *fl, const double *r1, const double *r2, const double *m1,
-                                           const double *m2, double *d, int rows)
+                                           const double *m2, double *d, int rows_)
 {
-#pragma unroll 2
+  const int rows = FULL ? SCAN_ROWS : rows_;
+#pragma unroll kScanUnroll
   for (int r = 0; r < rows; r += 2) {
     double2 xv[K], yv[K];
 #pragma unroll
@@ -272,7 +280,7 @@ __device__ __forceinline__ void scan_chunk(const double *const *xs, const double
     }
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
-      if (h == 1 && r + 1 >= rows) break;
+      if (!FULL && h == 1 && r + 1 >= rows) break;
 #pragma unroll
       for (int k = 0; k < K; ++k) {
         const double x = h ? xv[k].y : xv[k].x, y = h ? yv[k].y : yv[k].x;
@@ -414,17 +422,23 @@ k_hyp_pm(const State *st, const double *__restrict__ A, const int *__restrict__ 
     }
     const bool touch = __any_sync(0xFFFFFFFFu, mine);
     if (allfast) {
-      if (!touch) {
-        if (kw == 4) scan_chunk<4, true>(xs, ys, pr, qr, fl, r1, r2, m1, m2, d, rows);
-        else if (kw == 3) scan_chunk<3, true>(xs, ys, pr, qr, fl, r1, r2, m1, m2, d, rows);
-        else if (kw == 2) scan_chunk<2, true>(xs, ys, pr, qr, fl, r1, r2, m1, m2, d, rows);
-        else if (kw == 1) scan_chunk<1, true>(xs, ys, pr, qr, fl, r1, r2, m1, m2, d, rows);
+      if (!touch && rows == SCAN_ROWS) {
+        if (kw == 4) scan_chunk<4, true, true>(xs, ys, pr, qr, fl, r1, r2, m1, m2, d, rows);
+        else if (kw == 3) scan_chunk<3, true, true>(xs, ys, pr, qr, fl, r1, r2, m1, m2, d, rows);
+        else if (kw == 2) scan_chunk<2, true, true>(xs, ys, pr, qr, fl, r1, r2, m1, m2, d, rows);
+        else if (kw == 1) scan_chunk<1, true, true>(xs, ys, pr, qr, fl, r1, r2, m1, m2, d, rows);
+      }
+      else if (!touch) {
+        if (kw == 4) scan_chunk<4, true, false>(xs, ys, pr, qr, fl, r1, r2, m1, m2, d, rows);
+        else if (kw == 3) scan_chunk<3, true, false>(xs, ys, pr, qr, fl, r1, r2, m1, m2, d, rows);
+        else if (kw == 2) scan_chunk<2, true, false>(xs, ys, pr, qr, fl, r1, r2, m1, m2, d, rows);
+        else if (kw == 1) scan_chunk<1, true, false>(xs, ys, pr, qr, fl, r1, r2, m1, m2, d, rows);
       }
       else {
-        if (kw == 4) scan_chunk<4, false>(xs, ys, pr, qr, fl, r1, r2, m1, m2, d, rows);
-        else if (kw == 3) scan_chunk<3, false>(xs, ys, pr, qr, fl, r1, r2, m1, m2, d, rows);
-        else if (kw == 2) scan_chunk<2, false>(xs, ys, pr, qr, fl, r1, r2, m1, m2, d, rows);
-        else if (kw == 1) scan_chunk<1, false>(xs, ys, pr, qr, fl, r1, r2, m1, m2, d, rows);
+        if (kw == 4) scan_chunk<4, false, false>(xs, ys, pr, qr, fl, r1, r2, m1, m2, d, rows);
+        else if (kw == 3) scan_chunk<3, false, false>(xs, ys, pr, qr, fl, r1, r2, m1, m2, d, rows);
+        else if (kw == 2) scan_chunk<2, false, false>(xs, ys, pr, qr, fl, r1, r2, m1, m2, d, rows);
+        else if (kw == 1) scan_chunk<1, false, false>(xs, ys, pr, qr, fl, r1, r2, m1, m2, d, rows);
       }
     }
     else {
@@ -755,6 +769,7 @@ k_colsort(const State *st, const double *__restrict__ Wm, int n, unsigned short 
 {
   if (st->stop) return;
   __shared__ unsigned long long sk[SORT_THREADS * E];
+  __shared__ unsigned short slo[SORT_THREADS * E];  // low 16 bits of the sorted keys' weight keys
   __shared__ int s_cnt;
   const int v = blockIdx.x, tid = threadIdx.x;
   const int s2 = SORT_THREADS * E;
@@ -818,26 +833,42 @@ k_colsort(const State *st, const double *__restrict__ Wm, int n, unsigned short 
   for (int e = 0; e < E; ++e) sk[tid * E + e] = k[e];
   __syncthreads();
   const int cnt = s_cnt;
-  // runs of keys equal in their top 48 bits: order them by the full record order
-  for (int r = tid; r < cnt; r += blockDim.x) {
-    const unsigned long long h = sk[r] >> 16;
-    if ((r > 0 && (sk[r - 1] >> 16) == h) || r + 1 >= cnt || (sk[r + 1] >> 16) != h) continue;
-    int e = r + 1;
-    while (e + 1 < cnt && (sk[e + 1] >> 16) == h) ++e;
-    for (int i = r + 1; i <= e; ++i) {
-      const unsigned long long x = sk[i];
-      const unsigned long long fx = wkey(col[ckey_u(x, v)]);
-      int j = i - 1;
-      while (j >= r) {
-        const unsigned long long fy = wkey(col[ckey_u(sk[j], v)]);
-        if (fy > fx || (fy == fx && (sk[j] & 0xFFFFu) > (x & 0xFFFFu))) break;
-        sk[j + 1] = sk[j];
-        --j;
-      }
-      sk[j + 1] = x;
-    }
-  }
+  // the sort saw the top 48 bits of each weight key; keys that agree there but differ in
+  // the low 16 bits are in tie-code order and must be reordered by the full key.  The
+  // low bits of every sorted key, read in parallel, show whether any run needs it (near
+  // convergence many weights are exactly equal, zeros above all: those runs are already in
+  // the record order and are left alone).
+  for (int r = tid; r < cnt; r += blockDim.x) slo[r] = (unsigned short)(wkey(col[ckey_u(sk[r], v)]) & 0xFFFFu);
   __syncthreads();
+  int bad = 0;
+  for (int r = tid + 1; r < cnt; r += blockDim.x)
+    if ((sk[r] >> 16) == (sk[r - 1] >> 16) && slo[r] != slo[r - 1]) bad = 1;
+  if (__syncthreads_or(bad)) {
+    // each run of two or more keys with equal top bits and mixed low bits, by its head
+    // thread: insertion sort by (low bits, tie code), descending, in shared memory
+    for (int r = tid; r < cnt; r += blockDim.x) {
+      const unsigned long long h = sk[r] >> 16;
+      if ((r > 0 && (sk[r - 1] >> 16) == h) || r + 1 >= cnt || (sk[r + 1] >> 16) != h) continue;
+      int e = r + 1;
+      bool mixed = (slo[e] != slo[r]);
+      while (e + 1 < cnt && (sk[e + 1] >> 16) == h) { ++e; mixed = mixed || (slo[e] != slo[r]); }
+      if (!mixed) continue;
+      for (int i = r + 1; i <= e; ++i) {
+        const unsigned long long x = sk[i];
+        const unsigned short xl = slo[i];
+        const unsigned cx = ((unsigned)xl << 16) | (unsigned)(x & 0xFFFFu);
+        int j = i - 1;
+        while (j >= r && (((unsigned)slo[j] << 16) | (unsigned)(sk[j] & 0xFFFFu)) < cx) {
+          sk[j + 1] = sk[j];
+          slo[j + 1] = slo[j];
+          --j;
+        }
+        sk[j + 1] = x;
+        slo[j + 1] = xl;
+      }
+    }
+    __syncthreads();
+  }
   unsigned short *lv = list + (long long)v * list_ld(n);
   unsigned short *rv = rank + (long long)v * n;
   for (int r = tid; r < cnt; r += blockDim.x) {

@@ -154,6 +154,6 @@ def test_batched_gram_ranking_accurate():
     for m, (Y, Jm) in enumerate(zip(mats, Js)):
         ref, _ = oracle.accurate_sigma(Y, Jm, "q")
         sm = s[so[m]:so[m + 1]]
-        assert oracle.sigma_rel_err(sm, ref, Jm) <= 1e-12, m
+        assert oracle.sigma_rel_err(sm, ref, Jm) <= 1e-12, m  # iid Gaussian inputs
         assert np.linalg.norm(Us[m] @ np.diag(sm) @ Zs[m] - Y) <= 1e-12 * np.linalg.norm(Y), m
     assert abs(int(info.sum()) - int(res["exact"][0].sum())) <= 0.1 * res["exact"][0].sum()

