@@ -31,8 +31,9 @@ extern "C" {
 
 /* Options; a NULL pointer means all defaults (zero). */
 typedef struct {
-  int max_steps;    /* stop after this many steps (0: no limit, as DSTEP_LOOP, src/D/dstep.F90:564-578);
-                       INFO = JK_ERR_MAX_STEPS when hit, with A, U, Z, SIGMA as the loop left them */
+  int max_steps;    /* stop after this many steps (0: no limit, as DSTEP_LOOP, src/D/dstep.F90:564-578,
+                       except in the batched solver, see JK_BATCH_STEP_BOUND); INFO = JK_ERR_MAX_STEPS
+                       when hit, with A, U, Z, SIGMA as the loop left them */
   int zba_quirk;    /* complex BA branch of src/Z/ztransf.F90:325: 0 = as the reference (R1), 1 = R2 as the real code */
   int graph_steps;  /* steps per CUDA-graph launch (0: 32; -1: plain stream launches) */
   int device;       /* CUDA device ordinal for the host-pointer entry points (-1 or 0: current) */
@@ -167,8 +168,17 @@ int jk_dweights_noalloc(int n, const double *dA, const int *J, double *dW, void 
  * and SIGMA entries at sum_{k<m} n[k].  info[m] is the matrix's INFO (>= 0 steps, < 0
  * error).  Results equal jk_dstep_loop's on each matrix. */
 #define JK_BATCH_MAX_N 128
+/* The batched solver's step bound per matrix when opts->max_steps is 0: 4000 N_max + 100000
+ * (N_max the batch's largest order).  The reference loop has no bound, but some inputs
+ * practically never end: 7 of the 4096 matrices of the benchmark's batch (N in [16, 128])
+ * were still transforming after 2e7 steps, which keeps one SM busy for 14 minutes, and one
+ * persistent launch holds every matrix's results until its slowest matrix ends.  A matrix
+ * that reaches the bound returns INFO JK_ERR_MAX_STEPS with A, U, Z, SIGMA as its loop
+ * left them; jk_solver_resume continues it on the single-matrix loop, which has no bound. */
+#define JK_BATCH_STEP_BOUND(nmax) (4000LL * (nmax) + 100000LL)
 typedef struct jk_batch jk_batch;
-/* A plan for one batch shape (orders, N_2, J: host arrays); opts: max_steps, device. */
+/* A plan for one batch shape (orders, N_2, J: host arrays); opts: max_steps (0: the bound
+ * above), device. */
 jk_batch *jk_batch_create(int count, const int *n, const int *n_2, const int *J, const jk_opts *opts, int *info);
 void jk_batch_destroy(jk_batch *b);
 /* Enqueue the solve on device buffers (packed as above) on `stream`; A in/out, U, Z,

@@ -663,7 +663,7 @@ jk_batch *jk_batch_create(int count, const int *n, const int *n_2, const int *J,
     b->nm = nm;
     b->total = total;
     b->totaln = totaln;
-    b->cap = (opts && opts->max_steps > 0) ? opts->max_steps : (4000LL * nm + 100000LL);
+    b->cap = (opts && opts->max_steps > 0) ? opts->max_steps : JK_BATCH_STEP_BOUND(nm);
     // the work order: largest matrices first (the cost grows as N^4)
     std::vector<BatchItem> it(count);
     long long off = 0;
