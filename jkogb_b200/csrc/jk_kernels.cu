@@ -707,7 +707,9 @@ k_weights_hyp(const State *st, const T *__restrict__ A, const int *__restrict__ 
 // in registers, shuffles and shared memory), so a round only moves each free
 // vertex's list pointer past partners matched meanwhile (k_select, one block).
 // ---------------------------------------------------------------------------
-#define SEL_THREADS 1024
+#ifndef SEL_THREADS
+#define SEL_THREADS 1024  // threads of the one-block selection (a tuning knob)
+#endif
 #define SORT_THREADS 256
 
 // descending bitonic sort of s2 (a power of two) records (k, t, i) in shared memory
