@@ -286,10 +286,13 @@ __device__ __forceinline__ void scan_chunk(const double *const *xs, const double
         const double x = h ? xv[k].y : xv[k].x, y = h ? yv[k].y : yv[k].x;
         const double xx = __dmul_rn(fma(y, r1[k], x), m1[k]);
         const double yy = __dmul_rn(fma(x, r2[k], y), m2[k]);
-        const double e1 = fma(__dsub_rn(x, xx), __dadd_rn(x, xx), d[k]);
-        const double e2 = fma(__dsub_rn(y, yy), __dadd_rn(y, yy), e1);
-        if (FAST) d[k] = e2;  // inactive slots accumulate garbage that is never stored
-        else d[k] = ((fl[k] & 1) && (r + h) != pl[k] && (r + h) != ql[k]) ? e2 : d[k];
+        const double s1 = __dsub_rn(x, xx), a1 = __dadd_rn(x, xx), s2 = __dsub_rn(y, yy), a2 = __dadd_rn(y, yy);
+        if (FAST || ((r + h) != pl[k] && (r + h) != ql[k])) {
+          // inactive slots accumulate garbage that is never stored; a predicated pair of fmas
+          // instead of a select of their result
+          d[k] = fma(s1, a1, d[k]);
+          d[k] = fma(s2, a2, d[k]);
+        }
       }
     }
   }
@@ -711,6 +714,10 @@ k_weights_hyp(const State *st, const T *__restrict__ A, const int *__restrict__ 
 #define SEL_THREADS 1024  // threads of the one-block selection (a tuning knob)
 #endif
 #define SORT_THREADS 256
+#ifndef JK_SEL_CLUSTER_MIN_N
+#define JK_SEL_CLUSTER_MIN_N 512  // the cluster matching from this order on (a tuning knob)
+#endif
+constexpr int kSelClusterMinN = JK_SEL_CLUSTER_MIN_N;
 
 // descending bitonic sort of s2 (a power of two) records (k, t, i) in shared memory
 __device__ __forceinline__ void bitonic_desc(unsigned long long *k, unsigned *t, int *ix, int s2)
@@ -765,28 +772,13 @@ __device__ __forceinline__ int ckey_u(unsigned long long c, int v)
   return (t & 1) ? v + (t >> 1) : v - (t >> 1);
 }
 
+// descending bitonic sort of the SORT_THREADS * E keys a block holds E per thread
+// (position tid * E + e): stages with partner distance < E in registers, < 32 E by warp
+// shuffles, the rest through shared memory (sk, SORT_THREADS * E entries)
 template <int E>
-__global__ void __launch_bounds__(SORT_THREADS)
-k_colsort(const State *st, const double *__restrict__ Wm, int n, unsigned short *list, unsigned short *rank, int *len)
+__device__ __forceinline__ void block_sort_desc(unsigned long long (&k)[E], unsigned long long *sk)
 {
-  if (st->stop) return;
-  __shared__ unsigned long long sk[SORT_THREADS * E];
-  __shared__ unsigned short slo[SORT_THREADS * E];  // low 16 bits of the sorted keys' weight keys
-  __shared__ int s_cnt;
-  const int v = blockIdx.x, tid = threadIdx.x;
-  const int s2 = SORT_THREADS * E;
-  const double *col = Wm + (long long)v * n;
-  unsigned long long k[E];
-  int valid = 0;
-#pragma unroll
-  for (int e = 0; e < E; ++e) {
-    const int i = tid * E + e;
-    k[e] = (i < n && i != v) ? ckey(col[i], i, v) : 0ULL;
-    valid += k[e] ? 1 : 0;
-  }
-  if (tid == 0) s_cnt = 0;
-  __syncthreads();
-  atomicAdd(&s_cnt, valid);
+  const int tid = threadIdx.x, s2 = SORT_THREADS * E;
   for (int kk = 2; kk <= s2; kk <<= 1) {
     for (int j = kk >> 1; j >= E; j >>= 1) {
       if (j < 32 * E) {
@@ -830,45 +822,90 @@ k_colsort(const State *st, const double *__restrict__ Wm, int n, unsigned short 
       }
     }
   }
-  __syncthreads();
+}
+
+template <int E>
+__global__ void __launch_bounds__(SORT_THREADS)
+k_colsort(const State *st, const double *__restrict__ Wm, int n, unsigned short *list, unsigned short *rank, int *len)
+{
+  if (st->stop) return;
+  __shared__ unsigned long long sk[SORT_THREADS * E];
+  __shared__ unsigned short slo[SORT_THREADS * E];  // low 16 bits of the sorted keys' weight keys
+  __shared__ int s_cnt, s_warp[SORT_THREADS / 32];
+  const int v = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const double *col = Wm + (long long)v * n;
+  unsigned long long k[E];
+  int valid = 0;
 #pragma unroll
-  for (int e = 0; e < E; ++e) sk[tid * E + e] = k[e];
+  for (int e = 0; e < E; ++e) {
+    const int i = tid * E + e;
+    k[e] = (i < n && i != v) ? ckey(col[i], i, v) : 0ULL;
+    valid += k[e] ? 1 : 0;
+  }
+  if (tid == 0) s_cnt = 0;
+  __syncthreads();
+  atomicAdd(&s_cnt, valid);
+  block_sort_desc<E>(k, sk);
   __syncthreads();
   const int cnt = s_cnt;
-  // the sort saw the top 48 bits of each weight key; keys that agree there but differ in
-  // the low 16 bits are in tie-code order and must be reordered by the full key.  The
-  // low bits of every sorted key, read in parallel, show whether any run needs it (near
-  // convergence many weights are exactly equal, zeros above all: those runs are already in
-  // the record order and are left alone).
-  for (int r = tid; r < cnt; r += blockDim.x) slo[r] = (unsigned short)(wkey(col[ckey_u(sk[r], v)]) & 0xFFFFu);
+  // The sort saw the top 48 bits of each weight key: keys that agree there but differ in
+  // the low 16 bits are in tie-code order and must be reordered by the full key.  The low
+  // bits of every sorted key show whether any run of equal top bits needs it (near
+  // convergence many weights are exactly equal, zeros above all: such runs are already in
+  // the record order).
+  unsigned lo[E];
+#pragma unroll
+  for (int e = 0; e < E; ++e) {
+    const int i = tid * E + e;
+    sk[i] = k[e];
+    lo[e] = (i < cnt) ? (unsigned)(wkey(col[ckey_u(k[e], v)]) & 0xFFFFu) : 0u;
+    slo[i] = (unsigned short)lo[e];
+  }
   __syncthreads();
-  int bad = 0;
-  for (int r = tid + 1; r < cnt; r += blockDim.x)
-    if ((sk[r] >> 16) == (sk[r - 1] >> 16) && slo[r] != slo[r - 1]) bad = 1;
+  int bad = 0, starts = 0;
+  bool start[E];
+#pragma unroll
+  for (int e = 0; e < E; ++e) {
+    const int i = tid * E + e;
+    const bool same = (i > 0) && (i < cnt) && ((sk[i - 1] >> 16) == (k[e] >> 16));
+    start[e] = (i < cnt) && !same;
+    starts += start[e] ? 1 : 0;
+    if (same && slo[i - 1] != (unsigned short)lo[e]) bad = 1;
+  }
   if (__syncthreads_or(bad)) {
-    // each run of two or more keys with equal top bits and mixed low bits, by its head
-    // thread: insertion sort by (low bits, tie code), descending, in shared memory
-    for (int r = tid; r < cnt; r += blockDim.x) {
-      const unsigned long long h = sk[r] >> 16;
-      if ((r > 0 && (sk[r - 1] >> 16) == h) || r + 1 >= cnt || (sk[r + 1] >> 16) != h) continue;
-      int e = r + 1;
-      bool mixed = (slo[e] != slo[r]);
-      while (e + 1 < cnt && (sk[e + 1] >> 16) == h) { ++e; mixed = mixed || (slo[e] != slo[r]); }
-      if (!mixed) continue;
-      for (int i = r + 1; i <= e; ++i) {
-        const unsigned long long x = sk[i];
-        const unsigned short xl = slo[i];
-        const unsigned cx = ((unsigned)xl << 16) | (unsigned)(x & 0xFFFFu);
-        int j = i - 1;
-        while (j >= r && (((unsigned)slo[j] << 16) | (unsigned)(sk[j] & 0xFFFFu)) < cx) {
-          sk[j + 1] = sk[j];
-          slo[j + 1] = slo[j];
-          --j;
-        }
-        sk[j + 1] = x;
-        slo[j + 1] = xl;
-      }
+    // order every run by (low bits, tie code): a second sort on (run index, low 16 bits,
+    // tie code), the run index from a block-wide prefix count of the run starts
+    int c = starts;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int t = __shfl_up_sync(0xFFFFFFFFu, c, o);
+      if (lane >= o) c += t;
     }
+    if (lane == 31) s_warp[warp] = c;
+    __syncthreads();
+    if (warp == 0) {
+      int x = (lane < SORT_THREADS / 32) ? s_warp[lane] : 0;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(0xFFFFFFFFu, x, o);
+        if (lane >= o) x += t;
+      }
+      if (lane < SORT_THREADS / 32) s_warp[lane] = x;
+    }
+    __syncthreads();
+    int run = c - starts + (warp > 0 ? s_warp[warp - 1] : 0) - 1;  // the run before my first key
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      const int i = tid * E + e;
+      run += start[e] ? 1 : 0;
+      k[e] = (i < cnt) ? (((unsigned long long)(0xFFFFu - (unsigned)run) << 32) | ((unsigned long long)lo[e] << 16) |
+                          (k[e] & 0xFFFFull))
+                       : 0ULL;
+    }
+    block_sort_desc<E>(k, sk);  // the low 16 bits (the tie code, which names the partner) are kept
+    __syncthreads();
+#pragma unroll
+    for (int e = 0; e < E; ++e) sk[tid * E + e] = k[e];
     __syncthreads();
   }
   unsigned short *lv = list + (long long)v * list_ld(n);
@@ -923,15 +960,145 @@ __device__ void end_of_step(State *st, const Piv<T> *piv, const int *J, Trace &t
   }
 }
 
+// The walk of one free vertex's ranked partner list from its pointer to the first free
+// partner (-1: none left).  The vertex's window holds list entries wbase .. wbase + 15 in
+// shared memory, two 8-entry segments; once the pointer leaves the first segment, the
+// window slides by one segment and the segment after it is fetched with cp.async (it lands
+// while the round's barriers pass).  A pointer that runs past the window reads 32 entries
+// at a time with four independent loads.  lv indexes the vertex's own state.
+__device__ __forceinline__ int walk_list(const unsigned short *__restrict__ row, int lv, uint4 *win, unsigned short *ptr,
+                                         unsigned short *wbase, const unsigned short *slen, const unsigned char *ms)
+{
+  int p = ptr[lv], wb = wbase[lv];
+  const int L = slen[lv];
+  int found = -1;
+  while (p < L && found < 0) {
+    if (p < wb + 16) {
+      const int sg = (p - wb) >> 3;
+      const uint4 q4 = win[2 * lv + sg];
+      const unsigned w4[4] = { q4.x, q4.y, q4.z, q4.w };
+      const int a = wb + 8 * sg;
+#pragma unroll
+      for (int e = 0; e < 8; ++e) {
+        const int idx = a + e;
+        const int u = (int)((w4[e >> 1] >> ((e & 1) * 16)) & 0xFFFFu);
+        if (found < 0 && idx >= p && idx < L && !ms[u]) { found = u; p = idx; }
+      }
+      if (found < 0) p = a + 8;
+      continue;
+    }
+    // past the window: fetch the next 32 entries with four independent loads
+    const int a = p & ~7;
+    uint4 g4[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+      if (a + 8 * j < L) g4[j] = *(const uint4 *)(row + a + 8 * j);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      if (found >= 0 || a + 8 * j >= L) continue;
+      const unsigned w4[4] = { g4[j].x, g4[j].y, g4[j].z, g4[j].w };
+#pragma unroll
+      for (int e = 0; e < 8; ++e) {
+        const int idx = a + 8 * j + e;
+        const int u = (int)((w4[e >> 1] >> ((e & 1) * 16)) & 0xFFFFu);
+        if (found < 0 && idx >= p && idx < L && !ms[u]) { found = u; p = idx; }
+      }
+      if (found >= 0) {
+        // the window restarts at the segment of the find
+        wb = a + 8 * j;
+        win[2 * lv] = g4[j];
+        if (j < 3 && wb + 8 < L) win[2 * lv + 1] = g4[j + 1];
+        else if (wb + 8 < L) cp_async16(&win[2 * lv + 1], row + wb + 8);
+      }
+    }
+    if (found < 0) p = a + 32;
+  }
+  if (found < 0) p = L;
+  else if (p >= wb + 8 && p < wb + 16) {
+    // the first segment is used up: slide the window and fetch the segment after it
+    win[2 * lv] = win[2 * lv + 1];
+    wb += 8;
+    if (wb + 8 < L) cp_async16(&win[2 * lv + 1], row + wb + 8);
+  }
+  cp_async_commit();
+  ptr[lv] = (unsigned short)p;
+  wbase[lv] = (unsigned short)wb;
+  return found;
+}
+
+// a vertex's list state at the start of the matching
+__device__ __forceinline__ void walk_init(const unsigned short *__restrict__ row, int L, int lv, uint4 *win, unsigned short *ptr,
+                                          unsigned short *wbase, unsigned short *slen)
+{
+  ptr[lv] = 0;
+  wbase[lv] = 0;
+  slen[lv] = (unsigned short)L;
+  win[2 * lv] = ((const uint4 *)row)[0];
+  if (L > 8) win[2 * lv + 1] = ((const uint4 *)row)[1];
+}
+
+// By one block, after the matching: the matched pairs ranked by (weight key, tie key),
+// descending; the first N_2 are this step's pivots (the STEP array, rank order); the
+// columns outside them; the step's scalars.  ms is free scratch here.
+template <typename T>
+__device__ void select_finish(State *st, const double *__restrict__ Wm, int n, int n_2, int np, int rounds,
+                              const int2 *pairs, unsigned long long *skey, unsigned *stie, int *sidx, unsigned char *ms,
+                              Piv<T> *piv, int *unp, Trace &tr, int *s_nunp)
+{
+  const int tid = threadIdx.x, nth = blockDim.x;
+  const int s2 = pow2ceil(n / 2 > 0 ? n / 2 : 1);
+  for (int i = tid; i < s2; i += nth) {
+    if (i < np) {
+      const int2 pr = pairs[i];
+      skey[i] = wkey(Wm[(long long)pr.x * n + pr.y]);
+      stie[i] = tkey(pr.x, pr.y);
+      sidx[i] = i;
+    }
+    else { skey[i] = 0ULL; stie[i] = 0u; sidx[i] = -1; }
+  }
+  __syncthreads();
+  bitonic_desc(skey, stie, sidx, s2);
+  const int sl = (np < n_2) ? np : n_2;
+  for (int v = tid; v < n; v += nth) ms[v] = 0;
+  __syncthreads();
+  for (int r = tid; r < sl; r += nth) {
+    const int2 pr = pairs[sidx[r]];
+    ms[pr.x] = 1;
+    ms[pr.y] = 1;
+    Piv<T> &pv = piv[r];
+    pv.p = pr.x;
+    pv.q = pr.y;
+    pv.w = Wm[(long long)pr.x * n + pr.y];
+  }
+  __syncthreads();
+  for (int v = tid; v < n; v += nth)
+    if (!ms[v]) unp[atomicAdd(s_nunp, 1)] = v;
+  __syncthreads();
+  if (tid == 0) {
+    st->sl = sl;
+    st->nl = 0;
+    st->err = 0;
+    st->nunp = *s_nunp;
+    st->rounds = rounds;
+    if (sl <= 0) {
+      // DSTEP_EXEC returns with SL = 0: the loop ends with INFO = S (src/D/dstep.F90:421, 575-582)
+      st->info = st->steps;
+      st->stop = 1;
+      if (st->trace_on && st->trace_steps < st->trace_cap_steps) {
+        const int s = st->trace_steps++;
+        tr.sl[s] = 0; tr.nl[s] = -1; tr.tw[s] = -0.0; tr.trig[s] = 0; tr.hyp[s] = 0; tr.rounds[s] = rounds;
+      }
+    }
+    else st->pending = 1;
+  }
+}
+
 // one block: the end of the previous step, the matching rounds, the ranking of the
 // matched pairs and the first N_2 of them (the pivots of this step, rank order),
 // and the columns outside the pivot set.
 // A round is two barriers: (A) every free vertex finds its best free partner, the first
-// free entry of its ranked list from its pointer on; (B) mutual proposals are matched.
-// Each vertex keeps a window of 16 list entries in shared memory, two 8-entry segments;
-// once its pointer leaves the first segment, the window slides by one segment and the
-// next segment is fetched with cp.async, which lands while the round's barriers pass.
-// A pointer that runs past the window falls back to synchronous loads.
+// free entry of its ranked list from its pointer on (walk_list); (B) mutual proposals
+// are matched.
 template <typename T>
 __global__ void __launch_bounds__(SEL_THREADS, 1)
 k_select(State *st, const double *__restrict__ Wm, const int *__restrict__ J, int n, int n_2,
@@ -960,79 +1127,16 @@ k_select(State *st, const double *__restrict__ Wm, const int *__restrict__ J, in
   __syncthreads();
   if (s_stop) return;
   for (int v = tid; v < n; v += nth) {
-    const uint4 *row = (const uint4 *)(list + (long long)v * ld);
-    const int L = len[v];
     ms[v] = 0;
-    ptr[v] = 0;
-    wbase[v] = 0;
-    slen[v] = (unsigned short)L;
-    win[2 * v] = row[0];
-    if (L > 8) win[2 * v + 1] = row[1];
+    walk_init(list + (long long)v * ld, len[v], v, win, ptr, wbase, slen);
   }
   __syncthreads();
 
   for (int round = 0; round <= n / 2 + 1; ++round) {
     cp_async_wait<0>();  // this thread's window refills of the last round
     // phase A: the best free partner of every free vertex
-    for (int v = tid; v < n; v += nth) {
-      if (ms[v]) continue;
-      int p = ptr[v], wb = wbase[v];
-      const int L = slen[v];
-      const unsigned short *row = list + (long long)v * ld;
-      int found = -1;
-      while (p < L && found < 0) {
-        if (p < wb + 16) {
-          const int sg = (p - wb) >> 3;
-          const uint4 q4 = win[2 * v + sg];
-          const unsigned w4[4] = { q4.x, q4.y, q4.z, q4.w };
-          const int a = wb + 8 * sg;
-#pragma unroll
-          for (int e = 0; e < 8; ++e) {
-            const int idx = a + e;
-            const int u = (int)((w4[e >> 1] >> ((e & 1) * 16)) & 0xFFFFu);
-            if (found < 0 && idx >= p && idx < L && !ms[u]) { found = u; p = idx; }
-          }
-          if (found < 0) p = a + 8;
-          continue;
-        }
-        // past the window: fetch the next 32 entries with four independent loads
-        const int a = p & ~7;
-        uint4 g4[4];
-#pragma unroll
-        for (int j = 0; j < 4; ++j)
-          if (a + 8 * j < L) g4[j] = *(const uint4 *)(row + a + 8 * j);
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-          if (found >= 0 || a + 8 * j >= L) continue;
-          const unsigned w4[4] = { g4[j].x, g4[j].y, g4[j].z, g4[j].w };
-#pragma unroll
-          for (int e = 0; e < 8; ++e) {
-            const int idx = a + 8 * j + e;
-            const int u = (int)((w4[e >> 1] >> ((e & 1) * 16)) & 0xFFFFu);
-            if (found < 0 && idx >= p && idx < L && !ms[u]) { found = u; p = idx; }
-          }
-          if (found >= 0) {
-            // the window restarts at the segment of the find
-            wb = a + 8 * j;
-            win[2 * v] = g4[j];
-            if (j < 3 && wb + 8 < L) win[2 * v + 1] = g4[j + 1];
-            else if (wb + 8 < L) cp_async16(&win[2 * v + 1], row + wb + 8);
-          }
-        }
-        if (found < 0) p = a + 32;
-      }
-      if (found < 0) p = L;
-      else if (p >= wb + 8 && p < wb + 16) {
-        // the first segment is used up: slide the window and fetch the segment after it
-        win[2 * v] = win[2 * v + 1];
-        wb += 8;
-        if (wb + 8 < L) cp_async16(&win[2 * v + 1], row + wb + 8);
-      }
-      cp_async_commit();
-      ptr[v] = (unsigned short)p;
-      wbase[v] = (unsigned short)wb;
-      best[v] = found;
-    }
+    for (int v = tid; v < n; v += nth)
+      if (!ms[v]) best[v] = walk_list(list + (long long)v * ld, v, win, ptr, wbase, slen, ms);
     __syncthreads();
     // phase B: mutual proposals are matched; a vertex without a candidate retires
     int got = 0;
@@ -1051,55 +1155,111 @@ k_select(State *st, const double *__restrict__ Wm, const int *__restrict__ J, in
     if (!__syncthreads_or(got)) break;
   }
   cp_async_wait<0>();
+  select_finish<T>(st, Wm, n, n_2, s_cnt, s_rounds, pairs, skey, stie, sidx, ms, piv, unp, tr, &s_nunp);
+}
 
-  // rank the matched pairs: (weight key, tie key), descending
-  const int np = s_cnt;
-  for (int i = tid; i < s2; i += nth) {
-    if (i < np) {
-      const int2 pr = pairs[i];
-      skey[i] = wkey(Wm[(long long)pr.x * n + pr.y]);
-      stie[i] = tkey(pr.x, pr.y);
-      sidx[i] = i;
-    }
-    else { skey[i] = 0ULL; stie[i] = 0u; sidx[i] = -1; }
+// The same matching by a cluster of SEL_CLUSTER blocks sharing its state through
+// distributed shared memory (plain loads, stores and atomics; no multicast).  Block c owns
+// the vertices v = c (mod SEL_CLUSTER) and their list windows; every block keeps a replica
+// of every vertex's state (free, matched, retired), which phase B updates in all blocks.
+// A round: (A) every block walks its own free vertices' lists; cluster barrier; (B) a free
+// vertex whose best partner u proposes back (u's block holds best[u]) is matched with it,
+// the pair goes to block 0's list and both states change in every replica; cluster
+// barrier; every block reads the round's match count from block 0 and stops when it is 0.
+// Block 0 then ranks the matched pairs as the one-block kernel does.
+#define SEL_CLUSTER 8
+#define SEL_CTHREADS 256
+
+size_t select_cluster_smem(int n)
+{
+  const int s2 = pow2ceil(n / 2 > 0 ? n / 2 : 1);
+  const int np = (n / 2 + 1) + ((n / 2 + 1) & 1);
+  const int nl = (n + SEL_CLUSTER - 1) / SEL_CLUSTER;
+  return (size_t)s2 * (8 + 4 + 4) + (size_t)np * 8 + (size_t)nl * (32 + 4 + 2 + 2 + 2) + (size_t)n + 16;
+}
+
+template <typename T>
+__global__ void __cluster_dims__(SEL_CLUSTER, 1, 1) __launch_bounds__(SEL_CTHREADS, 1)
+k_select_cluster(State *st, const double *__restrict__ Wm, const int *__restrict__ J, int n, int n_2,
+                 const unsigned short *__restrict__ list, const int *__restrict__ len, Piv<T> *piv, int *unp, Trace tr)
+{
+  cg::cluster_group cluster = cg::this_cluster();
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int s2 = pow2ceil(n / 2 > 0 ? n / 2 : 1);
+  const int nl = (n + SEL_CLUSTER - 1) / SEL_CLUSTER;
+  unsigned long long *skey = (unsigned long long *)smem_raw;  // [s2]  (block 0)
+  unsigned *stie = (unsigned *)(skey + s2);                   // [s2]  (block 0)
+  int *sidx = (int *)(stie + s2);                             // [s2]  (block 0)
+  int2 *pairs = (int2 *)(sidx + s2);                          // [n/2 + 1]  (block 0)
+  uint4 *win = (uint4 *)(pairs + (n / 2 + 1) + ((n / 2 + 1) & 1)); // [nl][2]: own vertices' windows
+  int *best = (int *)(win + 2 * nl);                          // [nl]
+  unsigned short *ptr = (unsigned short *)(best + nl);        // [nl]
+  unsigned short *wbase = ptr + nl;                           // [nl]
+  unsigned short *slen = wbase + nl;                          // [nl]
+  unsigned char *ms = (unsigned char *)(slen + nl);           // [n]: replica of every vertex's state
+  __shared__ int s_stop, s_cnt, s_nunp, s_rounds, s_got[2];
+
+  const int tid = threadIdx.x, nth = blockDim.x, ld = list_ld(n);
+  const int c = (int)cluster.block_rank();
+  if (c == 0 && tid == 0) {
+    end_of_step<T>(st, piv, J, tr);
+    s_stop = st->stop;
+    s_cnt = 0; s_nunp = 0; s_rounds = 0; s_got[0] = 0; s_got[1] = 0;
   }
-  __syncthreads();
-  bitonic_desc(skey, stie, sidx, s2);
-  const int sl = (np < n_2) ? np : n_2;
-
-  // the pivot set and the columns outside it
   for (int v = tid; v < n; v += nth) ms[v] = 0;
-  __syncthreads();
-  for (int r = tid; r < sl; r += nth) {
-    const int2 pr = pairs[sidx[r]];
-    ms[pr.x] = 1;
-    ms[pr.y] = 1;
-    Piv<T> &pv = piv[r];
-    pv.p = pr.x;
-    pv.q = pr.y;
-    pv.w = Wm[(long long)pr.x * n + pr.y];
+  for (int lv = tid; lv * SEL_CLUSTER + c < n; lv += nth) {
+    const int v = lv * SEL_CLUSTER + c;
+    walk_init(list + (long long)v * ld, len[v], lv, win, ptr, wbase, slen);
   }
-  __syncthreads();
-  for (int v = tid; v < n; v += nth)
-    if (!ms[v]) unp[atomicAdd(&s_nunp, 1)] = v;
-  __syncthreads();
-  if (tid == 0) {
-    st->sl = sl;
-    st->nl = 0;
-    st->err = 0;
-    st->nunp = s_nunp;
-    st->rounds = s_rounds;
-    if (sl <= 0) {
-      // DSTEP_EXEC returns with SL = 0: the loop ends with INFO = S (src/D/dstep.F90:421, 575-582)
-      st->info = st->steps;
-      st->stop = 1;
-      if (st->trace_on && st->trace_steps < st->trace_cap_steps) {
-        const int s = st->trace_steps++;
-        tr.sl[s] = 0; tr.nl[s] = -1; tr.tw[s] = -0.0; tr.trig[s] = 0; tr.hyp[s] = 0; tr.rounds[s] = s_rounds;
+  int *got0 = cluster.map_shared_rank(s_got, 0);
+  int *cnt0 = cluster.map_shared_rank(&s_cnt, 0);
+  int2 *pairs0 = cluster.map_shared_rank(pairs, 0);
+  cluster.sync();
+  const int stop = *cluster.map_shared_rank(&s_stop, 0);
+  cluster.sync();  // every block has read block 0's flag
+  if (stop) return;
+
+  int rounds = 0;
+  for (int round = 0; round <= n / 2 + 1; ++round) {
+    cp_async_wait<0>();
+    // phase A: the best free partner of each own free vertex
+    for (int lv = tid; lv * SEL_CLUSTER + c < n; lv += nth) {
+      const int v = lv * SEL_CLUSTER + c;
+      if (!ms[v]) best[lv] = walk_list(list + (long long)v * ld, lv, win, ptr, wbase, slen, ms);
+    }
+    cluster.sync();
+    // the next round's match count starts at zero (every block read it two barriers ago)
+    if (c == 0 && tid == 0) s_got[(round + 1) & 1] = 0;
+    // phase B: mutual proposals are matched; a vertex without a candidate retires
+    int got = 0;
+    for (int lv = tid; lv * SEL_CLUSTER + c < n; lv += nth) {
+      const int v = lv * SEL_CLUSTER + c;
+      if (ms[v]) continue;
+      const int u = best[lv];
+      if (u < 0) {
+        for (int b = 0; b < SEL_CLUSTER; ++b) *cluster.map_shared_rank(&ms[v], b) = 2;
+        continue;
+      }
+      if (v < u && *cluster.map_shared_rank(&best[u / SEL_CLUSTER], u % SEL_CLUSTER) == v) {
+        for (int b = 0; b < SEL_CLUSTER; ++b) {
+          *cluster.map_shared_rank(&ms[v], b) = 1;
+          *cluster.map_shared_rank(&ms[u], b) = 1;
+        }
+        pairs0[atomicAdd(cnt0, 1)] = make_int2(v, u);
+        got += 1;
       }
     }
-    else st->pending = 1;
+    if (got) atomicAdd(&got0[round & 1], got);
+    cluster.sync();
+    rounds = round + 1;
+    if (!got0[round & 1]) {
+      cluster.sync();  // every block has read the count before block 0 goes on alone
+      break;
+    }
   }
+  cp_async_wait<0>();
+  if (c != 0) return;  // no block reads another's shared memory after the last barrier
+  select_finish<T>(st, Wm, n, n_2, s_cnt, rounds, pairs, skey, stie, sidx, ms, piv, unp, tr, &s_nunp);
 }
 
 // per pivot: the 2x2 HSVD of DSTEP_TRANSF's first loop (src/D/dstep.F90:301-326),
@@ -1478,6 +1638,9 @@ cudaError_t prepare_kernels(int n)
   const int ss = (int)select_smem(n);
   if (e == cudaSuccess) e = cudaFuncSetAttribute(k_select<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, ss);
   if (e == cudaSuccess) e = cudaFuncSetAttribute(k_select<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, ss);
+  const int cs = (int)select_cluster_smem(n);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_select_cluster<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, cs);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_select_cluster<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, cs);
   return e;
 }
 
@@ -1606,7 +1769,12 @@ static cudaError_t select_t(Workspace &w, const T *A, int n_2, cudaStream_t s)
   else {
     e = colsort(w, s);
     if (e != cudaSuccess) return e;
-    k_select<T><<<1, SEL_THREADS, select_smem(n), s>>>(w.st, w.Wm, w.J, n, n_2, w.list, w.len, (Piv<T> *)w.piv, w.unp, w.tr);
+    if (n >= kSelClusterMinN)
+      k_select_cluster<T><<<SEL_CLUSTER, SEL_CTHREADS, select_cluster_smem(n), s>>>(w.st, w.Wm, w.J, n, n_2, w.list, w.len,
+                                                                                  (Piv<T> *)w.piv, w.unp, w.tr);
+    else
+      k_select<T><<<1, SEL_THREADS, select_smem(n), s>>>(w.st, w.Wm, w.J, n, n_2, w.list, w.len, (Piv<T> *)w.piv, w.unp,
+                                                       w.tr);
   }
   if (A) {
     const int half = n / 2 > 0 ? n / 2 : 1;

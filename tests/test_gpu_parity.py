@@ -121,6 +121,29 @@ def test_select_random_ties(n):
             assert np.array_equal(jk.select(W, n2), oracle.select(n, w, P, Q, n2, id_ncp=2, nt=1)), (trial, n2)
 
 
+@pytest.mark.parametrize("n", [40, 300, 1000, 2100])
+def test_select_near_equal_weights(n):
+    """Weights that agree in the top 48 bits of their order key and differ only in the low
+    bits, mixed with exact ties and zeros: the partner ranking reorders those runs by the
+    full key (a second sort) and the selection equals the oracle's (orders of 512 and more
+    use the cluster matching; above 2048 the ranking holds sixteen keys per thread)."""
+    jk = _jk()
+    rng = np.random.Generator(np.random.PCG64(11 * n))
+    for trial in range(3):
+        P, Q, _ = oracle.pairs(n, np.ones(n, np.int32), 1)
+        base = np.array([1.0, 2.5, 0.0, 3.75])[rng.integers(0, 4, len(P))]
+        ulp = rng.integers(0, 2 ** 14, len(P)) * (trial > 0)   # low bits only (an order key's last 16)
+        w = (base.view(np.int64) + ulp).view(np.float64)
+        w[base == 0.0] = 0.0
+        if trial == 2:
+            w[rng.uniform(size=len(P)) < 0.3] = np.nan
+        W = np.full((n, n), np.nan)
+        W[P - 1, Q - 1] = w
+        W[Q - 1, P - 1] = w
+        for n2 in (n // 3, n // 2):
+            assert np.array_equal(jk.select(W, n2), oracle.select(n, w, P, Q, n2, id_ncp=2, nt=8)), (trial, n2)
+
+
 CASES = [
     # (kind, n, n_plus, n_2, seed)
     ("d", 3, 2, 0, 1), ("d", 4, 4, 0, 2), ("d", 5, 0, 0, 3), ("d", 8, 5, 0, 4), ("d", 16, 12, 3, 5),
