@@ -1,11 +1,15 @@
 """Run one named workload through the library on the current GPU.
 
-  python -m jkogb_b200.run WORKLOAD [--max-steps S] [--weights R]
+  python -m jkogb_b200.run WORKLOAD [--max-steps S] [--weights R] [--save-state F] [--load-state F]
   python -m jkogb_b200.run batch4096 [--matrices M] [--min-n K] [--max-steps S]
 
-Without --weights: one device-resident solve of the workload (jk_dstep_loop_dev /
-jk_zstep_loop_dev), stopped after S steps when --max-steps is given (the API's own step
-limit, INFO = -24), and prints INFO and the wall time.  With --weights R: R launches of
+Without --weights: one device-resident solve of the workload (jk_solver_*), stopped after S
+steps when --max-steps is given, and prints the steps, INFO and the wall time.  --save-state
+writes the loop's matrix (with its diagonal) where the run stopped to the .npy file F;
+--load-state starts the run from such a matrix instead of the workload's input, so that a
+profiler can look at a stretch deep inside the solve without replaying its start.  --ranking
+gram / learned: the scored solve (jk_dstep_loop_dev_scored) with the Gram form alone or with the
+trained network's correction.  With --weights R: R launches of
 one build's pair weights (jk_handle_weights) on the workload's input Y, the kernel-level
 form of the weight phase.  For the batched workload: one launch of the batched solver
 (jk_dstep_loop_batched) over its first M matrices of order >= K (all by default), each
@@ -29,6 +33,9 @@ def main(argv=None):
     ap.add_argument("--min-n", type=int, default=0)
     ap.add_argument("--max-steps", type=int, default=0)
     ap.add_argument("--weights", type=int, default=0)
+    ap.add_argument("--save-state", default="")
+    ap.add_argument("--load-state", default="")
+    ap.add_argument("--ranking", default="exact", choices=["exact", "gram", "learned"])
     a = ap.parse_args(argv)
 
     import torch
@@ -61,13 +68,32 @@ def main(argv=None):
         h.close()
         print(f"{a.workload}: {a.weights} weight launches in {time.perf_counter() - t0:.3f} s")
         return 0
-    A = Y0.clone().t().contiguous().t()
+    if a.load_state:
+        A = torch.from_numpy(np.ascontiguousarray(np.load(a.load_state).T)).to(dev).t().contiguous().t()
+    else:
+        A = Y0.clone().t().contiguous().t()
     U = torch.empty((n, n), dtype=tdt, device=dev).t()
     Z = torch.empty((n, n), dtype=tdt, device=dev).t()
     s = torch.empty(n, dtype=torch.float64, device=dev)
-    info = jk.step_loop_dev(A, U, Z, s, J, n_2=n_2, stream=stream, max_steps=a.max_steps)
+    if a.ranking != "exact":
+        from . import scorer
+        sc = scorer.Scorer(None if a.ranking == "gram" else scorer.load_params(), stall_k=8)
+        info, exact = sc.step_loop_dev(A, U, Z, s, J, n_2=n_2, stream=stream, max_steps=a.max_steps)
+        sc.close()
+        torch.cuda.synchronize(dev)
+        print(f"{a.workload} ({a.ranking}): INFO={info}, {exact} exact steps in {time.perf_counter() - t0:.3f} s")
+        return 0
+    sv = jk.Solver(n, J, n_2=n_2, complex_=cplx)
+    sv.begin(U.data_ptr(), A.data_ptr(), Z.data_ptr(), stream.cuda_stream)
+    sv.advance(a.max_steps)
+    steps = sv.steps
+    if a.save_state:
+        torch.cuda.synchronize(dev)
+        np.save(a.save_state, np.asfortranarray(A.cpu().numpy()))
+    info = sv.finish(s.data_ptr())
+    sv.close()
     torch.cuda.synchronize(dev)
-    print(f"{a.workload}: INFO={info} in {time.perf_counter() - t0:.3f} s")
+    print(f"{a.workload}: {steps} steps, INFO={info} in {time.perf_counter() - t0:.3f} s")
     return 0
 
 
