@@ -964,8 +964,10 @@ __device__ void end_of_step(State *st, const Piv<T> *piv, const int *J, Trace &t
 // partner (-1: none left).  The vertex's window holds list entries wbase .. wbase + 15 in
 // shared memory, two 8-entry segments; once the pointer leaves the first segment, the
 // window slides by one segment and the segment after it is fetched with cp.async (it lands
-// while the round's barriers pass).  A pointer that runs past the window reads 32 entries
-// at a time with four independent loads.  lv indexes the vertex's own state.
+// while the round's barriers pass).  A pointer that runs past the window reads 8 G entries
+// at a time with G independent 16-byte loads (a round takes as long as its longest walk, so
+// the round trips to memory count).  lv indexes the vertex's own state.
+template <int G>
 __device__ __forceinline__ int walk_list(const unsigned short *__restrict__ row, int lv, uint4 *win, unsigned short *ptr,
                                          unsigned short *wbase, const unsigned short *slen, const unsigned char *ms)
 {
@@ -987,14 +989,14 @@ __device__ __forceinline__ int walk_list(const unsigned short *__restrict__ row,
       if (found < 0) p = a + 8;
       continue;
     }
-    // past the window: fetch the next 32 entries with four independent loads
+    // past the window: fetch the next 8 G entries with G independent loads
     const int a = p & ~7;
-    uint4 g4[4];
+    uint4 g4[G];
 #pragma unroll
-    for (int j = 0; j < 4; ++j)
+    for (int j = 0; j < G; ++j)
       if (a + 8 * j < L) g4[j] = *(const uint4 *)(row + a + 8 * j);
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
+    for (int j = 0; j < G; ++j) {
       if (found >= 0 || a + 8 * j >= L) continue;
       const unsigned w4[4] = { g4[j].x, g4[j].y, g4[j].z, g4[j].w };
 #pragma unroll
@@ -1007,11 +1009,11 @@ __device__ __forceinline__ int walk_list(const unsigned short *__restrict__ row,
         // the window restarts at the segment of the find
         wb = a + 8 * j;
         win[2 * lv] = g4[j];
-        if (j < 3 && wb + 8 < L) win[2 * lv + 1] = g4[j + 1];
+        if (j < G - 1 && wb + 8 < L) win[2 * lv + 1] = g4[j + 1];
         else if (wb + 8 < L) cp_async16(&win[2 * lv + 1], row + wb + 8);
       }
     }
-    if (found < 0) p = a + 32;
+    if (found < 0) p = a + 8 * G;
   }
   if (found < 0) p = L;
   else if (p >= wb + 8 && p < wb + 16) {
@@ -1136,7 +1138,7 @@ k_select(State *st, const double *__restrict__ Wm, const int *__restrict__ J, in
     cp_async_wait<0>();  // this thread's window refills of the last round
     // phase A: the best free partner of every free vertex
     for (int v = tid; v < n; v += nth)
-      if (!ms[v]) best[v] = walk_list(list + (long long)v * ld, v, win, ptr, wbase, slen, ms);
+      if (!ms[v]) best[v] = walk_list<4>(list + (long long)v * ld, v, win, ptr, wbase, slen, ms);
     __syncthreads();
     // phase B: mutual proposals are matched; a vertex without a candidate retires
     int got = 0;
@@ -1225,7 +1227,7 @@ k_select_cluster(State *st, const double *__restrict__ Wm, const int *__restrict
     // phase A: the best free partner of each own free vertex
     for (int lv = tid; lv * SEL_CLUSTER + c < n; lv += nth) {
       const int v = lv * SEL_CLUSTER + c;
-      if (!ms[v]) best[lv] = walk_list(list + (long long)v * ld, lv, win, ptr, wbase, slen, ms);
+      if (!ms[v]) best[lv] = walk_list<16>(list + (long long)v * ld, lv, win, ptr, wbase, slen, ms);
     }
     cluster.sync();
     // the next round's match count starts at zero (every block read it two barriers ago)
