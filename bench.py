@@ -447,7 +447,7 @@ def run_ours(args, wl):
     # the learned form on the same input: the scored ranking (the trained network's
     # correction of the Gram form of the scanned weights), one device solve
     learned = None
-    if not cplx and os.path.exists(scorer_mod().PARAMS):
+    if os.path.exists(scorer_mod().PARAMS):
         sc = scorer_mod().Scorer(scorer_mod().load_params(), stall_k=8)
         A.copy_(Y0)
         barrier()

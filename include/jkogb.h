@@ -231,6 +231,15 @@ void jk_scorer_destroy(jk_scorer *sc);
  * that ranked by the exact weights. */
 int jk_dstep_loop_dev_scored(int n, double *dU, double *dA, double *dZ, const int *J, double *dsigma, int n_2,
                              const jk_scorer *sc, const jk_opts *opts, jk_trace *trace, int *exact_steps, void *stream);
+/* jk_zstep_loop_dev with the scored ranking (the complex weights of ZMAGF2H,
+ * src/Z/zstep.F90:43-74, whose scan ABODNZF2 sums |.|^2 of the complex entries): w_gram is
+ *   d + nx (1 - |Z11|^2 - |Z12|^2) + ny (1 - |Z21|^2 - |Z22|^2)
+ *     - 2 Re((conj(Z11) Z21 + conj(Z12) Z22) g),  g = x^H y,
+ * the real and imaginary parts of every x^H y from the same FP64 matrix product over the
+ * interleaved (re, im) columns; the network and its features are the real path's, with
+ * |g| for the product. */
+int jk_zstep_loop_dev_scored(int n, double *dU, double *dA, double *dZ, const int *J, double *dsigma, int n_2,
+                             const jk_scorer *sc, const jk_opts *opts, jk_trace *trace, int *exact_steps, void *stream);
 /* Training on the device.  jk_mlp_features writes the features of every hyperbolic pair
  * of the device matrix dA (step S = `step`) in (+ index, - index) order, the indices
  * ascending within each sign class, and returns their count; dWg (optional) receives each
@@ -241,6 +250,8 @@ int jk_dstep_loop_dev_scored(int n, double *dU, double *dA, double *dZ, const in
  * jk_mlp_grad_workspace(nf, count) floats.  jk_mlp_adam: one Adam update of the
  * parameters (step t >= 1). */
 long long jk_mlp_features(int n, const double *dA, const int *J, int step, float *dX, double *dWg, void *stream);
+/* jk_mlp_features of a complex device matrix (dA: N x N double complex, column-major). */
+long long jk_zmlp_features(int n, const double *dA, const int *J, int step, float *dX, double *dWg, void *stream);
 int jk_mlp_forward(int nf, int count, const float *dX, const float *dParams, float *dY, void *stream);
 long long jk_mlp_grad_workspace(int nf, int count);
 int jk_mlp_grad(int nf, int count, const float *dX, const float *dT, const float *dParams, float *dGrad, float *dLoss,

@@ -35,7 +35,8 @@ SYMBOLS = ("jk_dstep_loop", "jk_zstep_loop", "jk_dstep_loop_dev", "jk_zstep_loop
            "jk_zhsvd2_batch", "jk_dweights", "jk_zweights", "jk_select", "jk_handle_create", "jk_handle_destroy",
            "jk_handle_weights", "jk_dweights_noalloc", "jk_batch_create", "jk_batch_destroy",
            "jk_batch_run", "jk_batch_tune", "jk_batch_set_scorer", "jk_dstep_loop_batched", "jk_mlp_nparams", "jk_scorer_create",
-           "jk_scorer_destroy", "jk_dstep_loop_dev_scored", "jk_mlp_features", "jk_mlp_forward", "jk_mlp_grad_workspace",
+           "jk_scorer_destroy", "jk_dstep_loop_dev_scored", "jk_zstep_loop_dev_scored", "jk_mlp_features",
+           "jk_zmlp_features", "jk_mlp_forward", "jk_mlp_grad_workspace",
            "jk_mlp_grad", "jk_mlp_adam", "jk_last_launch_count", "jk_fp64_peak", "jk_max_order", "jk_strerror")
 
 
@@ -127,11 +128,13 @@ def lib():
         L.jk_scorer_create.argtypes = [C.c_int, C.POINTER(C.c_float), C.c_int, ip]
         L.jk_scorer_destroy.restype = None
         L.jk_scorer_destroy.argtypes = [C.c_void_p]
-        L.jk_dstep_loop_dev_scored.restype = C.c_int
-        L.jk_dstep_loop_dev_scored.argtypes = [C.c_int, vp, vp, vp, ip, vp, C.c_int, C.c_void_p, C.POINTER(Opts),
-                                               C.POINTER(Trace), ip, vp]
-        L.jk_mlp_features.restype = C.c_longlong
-        L.jk_mlp_features.argtypes = [C.c_int, vp, ip, C.c_int, vp, vp, vp]
+        for nm in ("jk_dstep_loop_dev_scored", "jk_zstep_loop_dev_scored"):
+            getattr(L, nm).restype = C.c_int
+            getattr(L, nm).argtypes = [C.c_int, vp, vp, vp, ip, vp, C.c_int, C.c_void_p, C.POINTER(Opts),
+                                       C.POINTER(Trace), ip, vp]
+        for nm in ("jk_mlp_features", "jk_zmlp_features"):
+            getattr(L, nm).restype = C.c_longlong
+            getattr(L, nm).argtypes = [C.c_int, vp, ip, C.c_int, vp, vp, vp]
         L.jk_mlp_forward.restype = C.c_int
         L.jk_mlp_forward.argtypes = [C.c_int, C.c_int, vp, vp, vp, vp]
         L.jk_mlp_grad_workspace.restype = C.c_longlong

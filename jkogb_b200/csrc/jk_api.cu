@@ -205,7 +205,7 @@ int solver_make(jk_solver *v, int cplx, int n, const int *J, int n_2, int id_ncp
     CK(g.alloc(&w.offcount, sizeof(int)));
     CK(cudaMemset(w.offcount, 0, sizeof(int)));
     // the Gram form of the scanned weights: the "+" x "-" column products, the column norms
-    CK(g.alloc(&w.gram, ((size_t)w.n_plus * w.n_minus + 1) * sizeof(double)));
+    CK(g.alloc(&w.gram, ((size_t)(cplx ? 2 : 1) * w.n_plus * w.n_minus + 1) * sizeof(double)));
     CK(g.alloc(&w.cn, (size_t)n * sizeof(double)));
     CK(prepare_gram());
   }
@@ -868,7 +868,17 @@ int jk_dstep_loop_dev_scored(int n, double *dU, double *dA, double *dZ, const in
   return run_loop(0, n, dU, dA, dZ, J, dsigma, n_2, 0, 0, opts, trace, (cudaStream_t)stream, sc, exact_steps);
 }
 
-long long jk_mlp_features(int n, const double *dA, const int *J, int step, float *dX, double *dWg, void *stream)
+int jk_zstep_loop_dev_scored(int n, double *dU, double *dA, double *dZ, const int *J, double *dsigma, int n_2,
+                             const jk_scorer *sc, const jk_opts *opts, jk_trace *trace, int *exact_steps, void *stream)
+{
+  if (!sc) return -9;
+  const int rc = check_args(n, n, n, n, J, n_2, 0, 0, 1);
+  if (rc) return rc;
+  return run_loop(1, n, dU, dA, dZ, J, dsigma, n_2, 0, 0, opts, trace, (cudaStream_t)stream, sc, exact_steps);
+}
+
+static long long features(int cplx, int n, const double *dA, const int *J, int step, float *dX, double *dWg,
+                          void *stream)
 {
   if (n < 3 || !dA || !J || !dX) return -1;
   std::vector<int> plus, minus;
@@ -886,7 +896,7 @@ long long jk_mlp_features(int n, const double *dA, const int *J, int step, float
   cudaStream_t s = (cudaStream_t)stream;
   CK(g.alloc(&dp, plus.size() * sizeof(int)));
   CK(g.alloc(&dm, minus.size() * sizeof(int)));
-  CK(g.alloc(&G, cnt * sizeof(double)));
+  CK(g.alloc(&G, (cplx ? 2 : 1) * cnt * sizeof(double)));
   CK(g.alloc(&cn, n * sizeof(double)));
   CK(g.alloc(&st, sizeof(State)));
   State s0;
@@ -895,9 +905,19 @@ long long jk_mlp_features(int n, const double *dA, const int *J, int step, float
   CK(cudaMemcpy(st, &s0, sizeof(State), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(dp, plus.data(), plus.size() * sizeof(int), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(dm, minus.data(), minus.size() * sizeof(int), cudaMemcpyHostToDevice));
-  CK(mlp_features(n, dA, dp, dm, (int)plus.size(), (int)minus.size(), step, st, G, cn, dX, dWg, s));
+  CK(mlp_features(cplx, n, dA, dp, dm, (int)plus.size(), (int)minus.size(), step, st, G, cn, dX, dWg, s));
   CK(cudaStreamSynchronize(s));  // the temporaries are freed on return
   return cnt;
+}
+
+long long jk_mlp_features(int n, const double *dA, const int *J, int step, float *dX, double *dWg, void *stream)
+{
+  return features(0, n, dA, J, step, dX, dWg, stream);
+}
+
+long long jk_zmlp_features(int n, const double *dA, const int *J, int step, float *dX, double *dWg, void *stream)
+{
+  return features(1, n, dA, J, step, dX, dWg, stream);
 }
 
 int jk_mlp_forward(int nf, int count, const float *dX, const float *dParams, float *dY, void *stream)

@@ -142,12 +142,12 @@ cudaError_t launch_batch(int variant, int grid, const BatchItem *items, int coun
 constexpr int kMlpHidden = 64;
 constexpr int kMlpFeat = 8;
 __host__ __device__ constexpr int mlp_params(int nf) { return kMlpHidden * nf + kMlpHidden + kMlpHidden * kMlpHidden + kMlpHidden + kMlpHidden + 1; }
-cudaError_t launch_learned_weights(Workspace &w, const double *A, cudaStream_t s);
+cudaError_t launch_learned_weights(Workspace &w, const void *A, cudaStream_t s);
 cudaError_t prepare_gram();
 constexpr int kOffBlocks = 296;  // fixed grid of the off-norm reduction (a fixed summation order)
-cudaError_t launch_offnorm(Workspace &w, const double *A, cudaStream_t s);
-cudaError_t mlp_features(int n, const double *A, const int *plus, const int *minus, int n_plus, int n_minus, int step,
-                         const State *st, double *G, double *cn, float *X, double *Wg, cudaStream_t s);
+cudaError_t launch_offnorm(Workspace &w, const void *A, cudaStream_t s);
+cudaError_t mlp_features(int cplx, int n, const void *A, const int *plus, const int *minus, int n_plus, int n_minus,
+                         int step, const State *st, double *G, double *cn, float *X, double *Wg, cudaStream_t s);
 cudaError_t mlp_forward(int nf, int count, const float *X, const unsigned short *w, const float *b, float *Y, cudaStream_t s);
 cudaError_t mlp_grad(int nf, int count, const float *X, const float *T, const float *params, float *grad, float *loss,
                      float *partial, cudaStream_t s);

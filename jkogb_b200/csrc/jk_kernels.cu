@@ -1796,19 +1796,15 @@ static cudaError_t step_t(Workspace &w, T *A, T *U, T *Z, int n_2, cudaStream_t 
   const int n = w.n;
   cudaError_t e = weights_t(w, (const T *)A, s);
   if (e != cudaSuccess) return e;
-  if constexpr (sizeof(T) == sizeof(double)) {
-    // a learned solve: the scorer ranks the scanned hyperbolic pairs (the exact scan
-    // kernels above return at once in its learned steps)
-    if (w.learned && (e = launch_learned_weights(w, (const double *)A, s)) != cudaSuccess) return e;
-  }
+  // a learned solve: the scorer ranks the scanned hyperbolic pairs (the exact scan kernels
+  // above return at once in its learned steps)
+  if (w.learned && (e = launch_learned_weights(w, A, s)) != cudaSuccess) return e;
   e = select_t(w, (const T *)A, n_2, s);
   if (e != cudaSuccess) return e;
   k_rotate<T><<<(n + 1) / 2, 256, 2 * (size_t)n * sizeof(T), s>>>(w.st, A, U, Z, n, (const Piv<T> *)w.piv,
                                                                  (const RowRot<T> *)w.rowrot, w.unp);
-  if constexpr (sizeof(T) == sizeof(double)) {
-    if (w.learned && (e = cudaGetLastError()) == cudaSuccess) e = launch_offnorm(w, (const double *)A, s);
-    if (e != cudaSuccess) return e;
-  }
+  if (w.learned && (e = cudaGetLastError()) == cudaSuccess) e = launch_offnorm(w, A, s);
+  if (e != cudaSuccess) return e;
   return cudaGetLastError();
 }
 

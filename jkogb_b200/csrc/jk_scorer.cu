@@ -161,17 +161,19 @@ __device__ __forceinline__ void mlp16(const TNet &s, const float (*xs)[NF], floa
 // the end-of-loop test stay exact.
 // ---------------------------------------------------------------------------
 
-// column off-diagonal norms cn[j] = sum_{i != j} A(i,j)^2 (one warp per column)
+// column off-diagonal norms cn[j] = sum_{i != j} |A(i,j)|^2 (one warp per column; C = 2:
+// complex A, each column read as 2 n interleaved reals)
+template <int C>
 __global__ void __launch_bounds__(256)
 k_colnorm(const State *st, const double *__restrict__ A, int n, double *__restrict__ cn)
 {
   if (st->stop || !st->learned_step) return;
   const int lane = threadIdx.x & 31;
   for (int j = blockIdx.x * 8 + (threadIdx.x >> 5); j < n; j += gridDim.x * 8) {
-    const double *c = A + (long long)j * n;
+    const double *c = A + (long long)j * C * n;
     double s = 0.0;
-    for (int i = lane; i < n; i += 32)
-      if (i != j) s = fma(c[i], c[i], s);
+    for (int i = lane; i < C * n; i += 32)
+      if (i / C != j) s = fma(c[i], c[i], s);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xFFFFFFFFu, s, o);
     if (!lane) cn[j] = s;
@@ -201,26 +203,30 @@ __device__ __forceinline__ void cp_async16g(void *smem, const void *gmem, bool f
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(gmem), "r"(sz));
 }
 
-__global__ void __launch_bounds__(128)
-k_gram(const State *st, const double *__restrict__ A, const int *__restrict__ plus, const int *__restrict__ minus,
-       int n_plus, int n_minus, int n, double *__restrict__ G)
+// C = 1: real A; C = 2: complex A, read as 2 n interleaved reals per column, so that the
+// real product of two columns is Re(x^H y); IM: the B operand's (re, im) pairs are read as
+// (im, -re), which makes the product Im(x^H y)
+template <int C, bool IM>
+__device__ __forceinline__ void gram_tile(const double *__restrict__ A, const int *__restrict__ plus,
+                                          const int *__restrict__ minus, int n_plus, int n_minus, int n,
+                                          double *__restrict__ G)
 {
-  if (st->stop || !st->learned_step) return;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   double (*xs)[GT][GKP] = (double (*)[GT][GKP])smem_raw;            // [2][GT][GKP]
   double (*ys)[GT][GKP] = (double (*)[GT][GKP])(smem_raw + kGramOperand);
   __shared__ int cx[GT], cy[GT];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int a0 = blockIdx.x * GT, b0 = blockIdx.y * GT;
+  const int nd = C * n;  // reals per column
   if (tid < GT) {
     cx[tid] = (a0 + tid < n_plus) ? plus[a0 + tid] : -1;
     cy[tid] = (b0 + tid < n_minus) ? minus[b0 + tid] : -1;
   }
   __syncthreads();
-  const int nk = (n + GK - 1) / GK;
-  // staging: 2 operands x 64 columns x 16 pieces of 16 bytes (two rows each) = 2048
-  // copies, 16 per thread; a piece that is not 16-byte aligned in A or runs past row n
-  // is loaded by plain loads (zeros past the end)
+  const int nk = (nd + GK - 1) / GK;
+  // staging: 2 operands x 64 columns x 16 pieces of 16 bytes (two reals each) = 2048
+  // copies, 16 per thread; a piece that is not 16-byte aligned in A or runs past the
+  // column's end is loaded by plain loads (zeros past the end)
   auto stage = [&](int c) {
     if (c < nk) {
       const int k0 = c * GK, buf = c & 1;
@@ -231,11 +237,11 @@ k_gram(const State *st, const double *__restrict__ A, const int *__restrict__ pl
         const int g = op ? cy[col] : cx[col];
         const int r = k0 + 2 * piece;
         double *dst = op ? &ys[buf][col][2 * piece] : &xs[buf][col][2 * piece];
-        const long long e = (long long)g * n + r;
-        if (g >= 0 && r + 1 < n && !(e & 1)) cp_async16g(dst, A + e, true);  // 16-byte aligned piece
+        const long long e = (long long)g * nd + r;
+        if (g >= 0 && r + 1 < nd && !(e & 1)) cp_async16g(dst, A + e, true);  // 16-byte aligned piece
         else {
-          dst[0] = (g >= 0 && r < n) ? A[e] : 0.0;
-          dst[1] = (g >= 0 && r + 1 < n) ? A[e + 1] : 0.0;
+          dst[0] = (g >= 0 && r < nd) ? A[e] : 0.0;
+          dst[1] = (g >= 0 && r + 1 < nd) ? A[e + 1] : 0.0;
         }
       }
     }
@@ -259,12 +265,16 @@ k_gram(const State *st, const double *__restrict__ A, const int *__restrict__ pl
     const int buf = c & 1, k0 = c * GK;
 #pragma unroll
     for (int kk = 0; kk < GK; kk += 4) {
-      const int row = k0 + kk + fk;  // the matrix row this lane's fragments hold
+      const int kr = kk + fk;             // this lane's real index in the chunk
+      const int row = (k0 + kr) / C;      // the matrix row it belongs to
       double fa[4], fb[4];
 #pragma unroll
       for (int i = 0; i < 4; ++i) {
-        fa[i] = (row == gxa[i]) ? 0.0 : xs[buf][wm + 8 * i + fr][kk + fk];
-        fb[i] = (row == gyb[i]) ? 0.0 : ys[buf][wn + 8 * i + fr][kk + fk];
+        fa[i] = (row == gxa[i]) ? 0.0 : xs[buf][wm + 8 * i + fr][kr];
+        double b;
+        if constexpr (IM) b = (kr & 1) ? -ys[buf][wn + 8 * i + fr][kr - 1] : ys[buf][wn + 8 * i + fr][kr + 1];
+        else b = ys[buf][wn + 8 * i + fr][kr];
+        fb[i] = (row == gyb[i]) ? 0.0 : b;
       }
 #pragma unroll
       for (int i = 0; i < 4; ++i)
@@ -288,6 +298,18 @@ k_gram(const State *st, const double *__restrict__ A, const int *__restrict__ pl
   }
 }
 
+// the Gram products of a scored step: G[a][b] (real A); Re and Im of x_a^H y_b (complex A,
+// blockIdx.z 0 and 1, the imaginary parts n_plus n_minus entries after the real ones)
+template <int C>
+__global__ void __launch_bounds__(128)
+k_gram(const State *st, const double *__restrict__ A, const int *__restrict__ plus, const int *__restrict__ minus,
+       int n_plus, int n_minus, int n, double *__restrict__ G)
+{
+  if (st->stop || !st->learned_step) return;
+  if (C == 2 && blockIdx.z) gram_tile<C, true>(A, plus, minus, n_plus, n_minus, n, G + (long long)n_plus * n_minus);
+  else gram_tile<C, false>(A, plus, minus, n_plus, n_minus, n, G);
+}
+
 
 
 // ---------------------------------------------------------------------------
@@ -300,7 +322,7 @@ struct GPair {
   float x[NF];  // features of a scanned pair
 };
 
-__device__ __forceinline__ GPair gram_pair(const double *__restrict__ A, int n, int a, int b, long long gidx,
+__device__ __forceinline__ GPair gram_pair(const double *__restrict__ A, int n, int a, int b, long long gidx, long long,
                                            const double *__restrict__ G, const double *__restrict__ cn, int step)
 {
   GPair r;
@@ -342,13 +364,65 @@ __device__ __forceinline__ GPair gram_pair(const double *__restrict__ A, int n, 
   return r;
 }
 
+// the complex pair (ZMAGF2H, src/Z/zstep.F90:43-74): with x, y the columns p, q without
+// rows p, q and g = x^H y (the Gram product of the "+" and "-" columns, conjugated when the
+// "-" column comes first), the scan's sum is d + nx (1 - |Z11|^2 - |Z12|^2) +
+// ny (1 - |Z21|^2 - |Z22|^2) - 2 Re((conj(Z11) Z21 + conj(Z12) Z22) g)
+__device__ __forceinline__ GPair gram_pair(const double2 *__restrict__ A, int n, int a, int b, long long gidx,
+                                           long long npm, const double *__restrict__ G, const double *__restrict__ cn,
+                                           int step)
+{
+  GPair r;
+  r.w = nan_w();
+  r.scan = 0;
+  const bool a_is_p = a < b;
+  const int p = a_is_p ? a : b, q = a_is_p ? b : a;
+  const double2 app = A[(long long)p * n + p], aqp = A[(long long)p * n + q], apq = A[(long long)q * n + p],
+                aqq = A[(long long)q * n + q];
+  if (!may_transform(app, aqp, apq, aqq)) return r;
+  double2 A2[4] = { app, aqp, apq, aqq }, U2[4], Z2[4];
+  int info = 0;
+  const int jp = a_is_p ? 1 : -1;
+  zhsvd2(A2, jp, -jp, U2, Z2, JK_TH1FIX, info);
+  if (info < 0) return r;
+  if (!(info & 1)) { r.w = 0.0; return r; }
+  if (!(info & 4)) { r.w = dasum4(aqp.x, aqp.y, apq.x, apq.y); return r; }
+  const double2 a1 = (info & 8) ? A2[M21] : make_double2(0.0, 0.0);
+  const double2 a2 = (info & 8) ? A2[M12] : make_double2(0.0, 0.0);
+  double d = 0.0;
+  d = fma(__dsub_rn(aqp.x, a1.x), __dadd_rn(aqp.x, a1.x), d);
+  d = fma(__dsub_rn(aqp.y, a1.y), __dadd_rn(aqp.y, a1.y), d);
+  d = fma(__dsub_rn(apq.x, a2.x), __dadd_rn(apq.x, a2.x), d);
+  d = fma(__dsub_rn(apq.y, a2.y), __dadd_rn(apq.y, a2.y), d);
+  const double2 z11 = Z2[M11], z21 = Z2[M21], z12 = Z2[M12], z22 = Z2[M22];
+  const double nx = cn[p] - (aqp.x * aqp.x + aqp.y * aqp.y), ny = cn[q] - (apq.x * apq.x + apq.y * apq.y);
+  const double gr = G[gidx], gi = a_is_p ? G[npm + gidx] : -G[npm + gidx];
+  const double c1 = (1.0 - z11.x) * (1.0 + z11.x) - z11.y * z11.y - (z12.x * z12.x + z12.y * z12.y);
+  const double c2 = (1.0 - z22.x) * (1.0 + z22.x) - z22.y * z22.y - (z21.x * z21.x + z21.y * z21.y);
+  // c3 = conj(z11) z21 + conj(z12) z22
+  const double c3r = (z11.x * z21.x + z11.y * z21.y) + (z12.x * z22.x + z12.y * z22.y);
+  const double c3i = (z11.x * z21.y - z11.y * z21.x) + (z12.x * z22.y - z12.y * z22.x);
+  r.w = d + (nx * c1 + ny * c2 - 2.0 * (c3r * gr - c3i * gi));
+  r.scan = 1;
+  r.x[0] = bf16_round(lg64(r.w));
+  r.x[1] = (r.w < 0.0) ? -1.0f : 1.0f;
+  r.x[2] = bf16_round(lg64(nx));
+  r.x[3] = bf16_round(lg64(ny));
+  r.x[4] = bf16_round(lg64(hypot(gr, gi)));
+  r.x[5] = bf16_round(lg64(d));
+  r.x[6] = bf16_round(lg64(zabs(z12) + zabs(z21)));
+  r.x[7] = bf16_round(fminf((float)step / (10.0f * (float)n), 4.0f));
+  return r;
+}
+
 // the score of a scanned pair from the network's output
 __device__ __forceinline__ double corrected(double w, float y) { return w * exp2((double)fminf(fmaxf(y, -1.0f), 1.0f) * 0.125); }
 
 // the weights of the hyperbolic pairs in a scored step (one thread per pair, (+, -) order);
 // with a network, every warp scores its 32 pairs as two tiles of 16 on the tensor cores
+template <typename T>
 __global__ void __launch_bounds__(256)
-k_hyp_gram(const State *st, const double *__restrict__ A, const int *__restrict__ plus, const int *__restrict__ minus,
+k_hyp_gram(const State *st, const T *__restrict__ A, const int *__restrict__ plus, const int *__restrict__ minus,
            int n_plus, int n_minus, int n, const double *__restrict__ G, const double *__restrict__ cn,
            double *__restrict__ Wm, ScorerDev sc)
 {
@@ -369,7 +443,8 @@ k_hyp_gram(const State *st, const double *__restrict__ A, const int *__restrict_
   if (valid) {
     ia = (int)(k / n_minus);
     ib = (int)(k % n_minus);
-    r = gram_pair(A, n, plus[ia], minus[ib], (long long)ia * n_minus + ib, G, cn, st->steps);
+    r = gram_pair(A, n, plus[ia], minus[ib], (long long)ia * n_minus + ib, (long long)n_plus * n_minus, G, cn,
+                  st->steps);
   }
   if (with_net && __any_sync(0xFFFFFFFFu, r.scan)) {
 #pragma unroll
@@ -391,15 +466,16 @@ k_hyp_gram(const State *st, const double *__restrict__ A, const int *__restrict_
 
 // training data: the features and w_gram of every hyperbolic pair ((+, -) order); the
 // pairs that need no scan get zero features and a NaN w_gram
+template <typename T>
 __global__ void __launch_bounds__(256)
-k_gram_features(const double *__restrict__ A, const int *__restrict__ plus, const int *__restrict__ minus, int n_plus,
+k_gram_features(const T *__restrict__ A, const int *__restrict__ plus, const int *__restrict__ minus, int n_plus,
                 int n_minus, int n, const double *__restrict__ G, const double *__restrict__ cn, int step, float *X,
                 double *Wg)
 {
   const long long k = blockIdx.x * 256LL + threadIdx.x;
   if (k >= (long long)n_plus * n_minus) return;
   const int ia = (int)(k / n_minus), ib = (int)(k % n_minus);
-  const GPair r = gram_pair(A, n, plus[ia], minus[ib], k, G, cn, step);
+  const GPair r = gram_pair(A, n, plus[ia], minus[ib], k, (long long)n_plus * n_minus, G, cn, step);
 #pragma unroll
   for (int f = 0; f < NF; ++f) X[k * NF + f] = r.scan ? r.x[f] : 0.0f;
   if (Wg) Wg[k] = r.scan ? r.w : nan_w();
@@ -408,8 +484,12 @@ k_gram_features(const double *__restrict__ A, const int *__restrict__ plus, cons
 // the off-norm sum_{i != j} A(i,j)^2 after a scored step, in a fixed summation order
 // (per-block tree sums, then the last block adds the block sums in block order), and
 // the choice of the next step's ranking
+__device__ __forceinline__ double sq_acc(double a, double acc) { return fma(a, a, acc); }
+__device__ __forceinline__ double sq_acc(double2 a, double acc) { return fma(a.y, a.y, fma(a.x, a.x, acc)); }
+
+template <typename T>
 __global__ void __launch_bounds__(256)
-k_offnorm(State *st, const double *__restrict__ A, int n, double *part, int *count)
+k_offnorm(State *st, const T *__restrict__ A, int n, double *part, int *count)
 {
   if (st->stop || !st->learned) return;
   __shared__ double red[256];
@@ -418,7 +498,7 @@ k_offnorm(State *st, const double *__restrict__ A, int n, double *part, int *cou
   double acc = 0.0;
   for (long long k = blockIdx.x * 256LL + threadIdx.x; k < nn; k += (long long)gridDim.x * 256) {
     const int i = (int)(k % n), j = (int)(k / n);
-    if (i != j) acc = fma(A[k], A[k], acc);
+    if (i != j) acc = sq_acc(A[k], acc);
   }
   red[threadIdx.x] = acc;
   __syncthreads();
@@ -660,43 +740,65 @@ __global__ void k_mlp_pack(const float *__restrict__ P, unsigned short *w, float
 // ---------------------------------------------------------------------------
 // host launchers
 // ---------------------------------------------------------------------------
-cudaError_t launch_learned_weights(Workspace &w, const double *A, cudaStream_t s)
+template <typename T>
+static cudaError_t learned_weights_t(Workspace &w, const T *A, cudaStream_t s)
 {
+  constexpr int C = sizeof(T) / sizeof(double);
   if (w.n_plus > 0 && w.n_minus > 0) {
     const int n = w.n;
-    k_colnorm<<<(n + 7) / 8 < 1184 ? (n + 7) / 8 : 1184, 256, 0, s>>>(w.st, A, n, w.cn);
-    dim3 g((w.n_plus + GT - 1) / GT, (w.n_minus + GT - 1) / GT);
-    k_gram<<<g, 128, 2 * kGramOperand, s>>>(w.st, A, w.plus, w.minus, w.n_plus, w.n_minus, n, w.gram);
+    k_colnorm<C><<<(n + 7) / 8 < 1184 ? (n + 7) / 8 : 1184, 256, 0, s>>>(w.st, (const double *)A, n, w.cn);
+    dim3 g((w.n_plus + GT - 1) / GT, (w.n_minus + GT - 1) / GT, C);
+    k_gram<C><<<g, 128, 2 * kGramOperand, s>>>(w.st, (const double *)A, w.plus, w.minus, w.n_plus, w.n_minus, n, w.gram);
     const long long np = (long long)w.n_plus * w.n_minus;
-    k_hyp_gram<<<(unsigned)((np + 255) / 256), 256, 0, s>>>(w.st, A, w.plus, w.minus, w.n_plus, w.n_minus, n, w.gram,
-                                                           w.cn, w.Wm, w.sc);
+    k_hyp_gram<T><<<(unsigned)((np + 255) / 256), 256, 0, s>>>(w.st, A, w.plus, w.minus, w.n_plus, w.n_minus, n,
+                                                              w.gram, w.cn, w.Wm, w.sc);
   }
   return cudaGetLastError();
 }
 
-cudaError_t prepare_gram()
+cudaError_t launch_learned_weights(Workspace &w, const void *A, cudaStream_t s)
 {
-  return cudaFuncSetAttribute(k_gram, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(2 * kGramOperand));
+  return w.cplx ? learned_weights_t(w, (const double2 *)A, s) : learned_weights_t(w, (const double *)A, s);
 }
 
-cudaError_t launch_offnorm(Workspace &w, const double *A, cudaStream_t s)
+cudaError_t prepare_gram()
 {
-  k_offnorm<<<kOffBlocks, 256, 0, s>>>(w.st, A, w.n, w.offpart, w.offcount);
+  const int sm = (int)(2 * kGramOperand);
+  cudaError_t e = cudaFuncSetAttribute(k_gram<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_gram<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  return e;
+}
+
+cudaError_t launch_offnorm(Workspace &w, const void *A, cudaStream_t s)
+{
+  if (w.cplx) k_offnorm<double2><<<kOffBlocks, 256, 0, s>>>(w.st, (const double2 *)A, w.n, w.offpart, w.offcount);
+  else k_offnorm<double><<<kOffBlocks, 256, 0, s>>>(w.st, (const double *)A, w.n, w.offpart, w.offcount);
   return cudaGetLastError();
 }
 
-cudaError_t mlp_features(int n, const double *A, const int *plus, const int *minus, int n_plus, int n_minus, int step,
-                         const State *st, double *G, double *cn, float *X, double *Wg, cudaStream_t s)
+template <typename T>
+static cudaError_t features_t(int n, const T *A, const int *plus, const int *minus, int n_plus, int n_minus, int step,
+                              const State *st, double *G, double *cn, float *X, double *Wg, cudaStream_t s)
+{
+  constexpr int C = sizeof(T) / sizeof(double);
+  const long long cnt = (long long)n_plus * n_minus;
+  k_colnorm<C><<<(n + 7) / 8 < 1184 ? (n + 7) / 8 : 1184, 256, 0, s>>>(st, (const double *)A, n, cn);
+  dim3 g((n_plus + GT - 1) / GT, (n_minus + GT - 1) / GT, C);
+  k_gram<C><<<g, 128, 2 * kGramOperand, s>>>(st, (const double *)A, plus, minus, n_plus, n_minus, n, G);
+  k_gram_features<T><<<(unsigned)((cnt + 255) / 256), 256, 0, s>>>(A, plus, minus, n_plus, n_minus, n, G, cn, step, X,
+                                                                    Wg);
+  return cudaGetLastError();
+}
+
+cudaError_t mlp_features(int cplx, int n, const void *A, const int *plus, const int *minus, int n_plus, int n_minus,
+                         int step, const State *st, double *G, double *cn, float *X, double *Wg, cudaStream_t s)
 {
   const long long cnt = (long long)n_plus * n_minus;
   if (cnt <= 0) return cudaSuccess;
   cudaError_t e = prepare_gram();
   if (e != cudaSuccess) return e;
-  k_colnorm<<<(n + 7) / 8 < 1184 ? (n + 7) / 8 : 1184, 256, 0, s>>>(st, A, n, cn);
-  dim3 g((n_plus + GT - 1) / GT, (n_minus + GT - 1) / GT);
-  k_gram<<<g, 128, 2 * kGramOperand, s>>>(st, A, plus, minus, n_plus, n_minus, n, G);
-  k_gram_features<<<(unsigned)((cnt + 255) / 256), 256, 0, s>>>(A, plus, minus, n_plus, n_minus, n, G, cn, step, X, Wg);
-  return cudaGetLastError();
+  return cplx ? features_t(n, (const double2 *)A, plus, minus, n_plus, n_minus, step, st, G, cn, X, Wg, s)
+              : features_t(n, (const double *)A, plus, minus, n_plus, n_minus, step, st, G, cn, X, Wg, s);
 }
 
 cudaError_t mlp_forward(int nf, int count, const float *X, const unsigned short *w, const float *b, float *Y, cudaStream_t s)

@@ -57,9 +57,9 @@ def _stream(torch, dev):
 
 
 def features(dA, J, step):
-    """Features of every hyperbolic pair of the column-major device matrix dA (torch),
-    (+ index, - index) order; returns (X (count, 8) float32 on the device, w_gram (count)
-    float64 on the device, NaN for the pairs that need no scan, plus, minus)."""
+    """Features of every hyperbolic pair of the column-major device matrix dA (torch, float64
+    or complex128), (+ index, - index) order; returns (X (count, 8) float32 on the device,
+    w_gram (count) float64 on the device, NaN for the pairs that need no scan, plus, minus)."""
     import torch
     n = dA.shape[0]
     Jc = np.ascontiguousarray(np.asarray(J, np.int32))
@@ -68,8 +68,8 @@ def features(dA, J, step):
     m = max(len(plus) * len(minus), 1)
     X = torch.empty((m, NF), dtype=torch.float32, device=dA.device)
     Wg = torch.empty(m, dtype=torch.float64, device=dA.device)
-    cnt = lib().jk_mlp_features(n, _vp(dA), Jc.ctypes.data_as(C.POINTER(C.c_int)), int(step), _vp(X), _vp(Wg),
-                                _stream(torch, dA.device))
+    f = lib().jk_zmlp_features if dA.dtype == torch.complex128 else lib().jk_mlp_features
+    cnt = f(n, _vp(dA), Jc.ctypes.data_as(C.POINTER(C.c_int)), int(step), _vp(X), _vp(Wg), _stream(torch, dA.device))
     if cnt < 0:
         raise JkError(int(cnt), "features: ")
     return X[:cnt], Wg[:cnt], plus, minus
@@ -185,18 +185,20 @@ class Scorer:
             raise JkError(info.value, "scorer: ")
 
     def step_loop_dev(self, A, U, Z, sigma, J, n_2=0, stream=None, max_steps=0):
-        """jk_dstep_loop_dev_scored on column-major torch tensors; returns (INFO, exact steps)."""
+        """jk_dstep_loop_dev_scored (float64) or jk_zstep_loop_dev_scored (complex128) on
+        column-major torch tensors; returns (INFO, exact steps)."""
         import torch
         n = A.shape[0]
+        assert A.dtype in (torch.float64, torch.complex128)
         for t in (A, U, Z):
-            assert t.is_cuda and t.dtype == torch.float64 and t.shape == (n, n) and t.stride() == (1, n)
+            assert t.is_cuda and t.dtype == A.dtype and t.shape == (n, n) and t.stride() == (1, n)
         Jc = np.ascontiguousarray(np.asarray(J).astype(np.int32))
         o = _opts(max_steps, 0, 0, A.device.index or 0)
         st = stream if stream is not None else torch.cuda.current_stream(A.device)
         ex = C.c_int(0)
-        info = lib().jk_dstep_loop_dev_scored(n, U.data_ptr(), A.data_ptr(), Z.data_ptr(),
-                                              Jc.ctypes.data_as(C.POINTER(C.c_int)), sigma.data_ptr(), int(n_2), self._s,
-                                              C.byref(o), None, C.byref(ex), C.c_void_p(st.cuda_stream))
+        f = lib().jk_zstep_loop_dev_scored if A.dtype == torch.complex128 else lib().jk_dstep_loop_dev_scored
+        info = f(n, U.data_ptr(), A.data_ptr(), Z.data_ptr(), Jc.ctypes.data_as(C.POINTER(C.c_int)), sigma.data_ptr(),
+                 int(n_2), self._s, C.byref(o), None, C.byref(ex), C.c_void_p(st.cuda_stream))
         if info < 0 and info != -24:
             raise JkError(info, "scored step loop: ")
         return info, ex.value

@@ -46,9 +46,14 @@ def features(A, J, step):
       w_gram = d0 + nx (1 - Z11^2 - Z12^2) + ny (1 - Z21^2 - Z22^2) - 2 (Z11 Z21 + Z12 Z22) g,
     nx = x.x, ny = y.y, g = x.y, d0 the two leading terms of ABODNDF2; the features are the
     BF16 roundings of log2/64 of |w_gram|, nx, ny, |g|, |d0|, |Z12| + |Z21|, sign(w_gram) and
-    min(S / (10 N), 4).  Other pairs: zero features and w_gram NaN.  Returns (X, w_gram)."""
+    min(S / (10 N), 4).  Other pairs: zero features and w_gram NaN.  Returns (X, w_gram).
+    A complex A (jk_zmlp_features, ZMAGF2H / ABODNZF2): nx = x^H x, ny = y^H y, g = x^H y,
+    d0 over the real and imaginary parts of the two leading terms and
+      w_gram = d0 + nx (1 - |Z11|^2 - |Z12|^2) + ny (1 - |Z21|^2 - |Z22|^2)
+               - 2 Re((conj(Z11) Z21 + conj(Z12) Z22) g)."""
     import oracle
-    A = np.asarray(A, np.float64)
+    cplx = np.iscomplexobj(A)
+    A = np.asarray(A, np.complex128 if cplx else np.float64)
     n = A.shape[0]
     J = np.asarray(J)
     plus = np.nonzero(J == 1)[0]
@@ -64,25 +69,41 @@ def features(A, J, step):
             p, q = (a, b) if a < b else (b, a)
             jp = 1 if a < b else -1
             app, aqp, apq, aqq = A[p, p], A[q, p], A[p, q], A[q, q]
-            if not (aqp != 0 or apq != 0 or np.signbit(app) or np.signbit(aqq)):
+            if cplx:
+                may = aqp != 0 or apq != 0 or app.imag != 0 or aqq.imag != 0 or np.signbit(app.real) or \
+                    np.signbit(aqq.real)
+            else:
+                may = aqp != 0 or apq != 0 or np.signbit(app) or np.signbit(aqq)
+            if not may:
                 continue
             A2, U2, Z2, info = oracle.hsvd2(np.array([[app, apq], [aqp, aqq]]), [jp, -jp])
             if info < 0 or not (info & 1) or not (info & 4):
                 continue
             a1 = A2[1, 0] if info & 8 else 0.0
             a2 = A2[0, 1] if info & 8 else 0.0
-            d = (aqp - a1) * (aqp + a1) + (apq - a2) * (apq + a2)
             z11, z21, z12, z22 = Z2[0, 0], Z2[1, 0], Z2[0, 1], Z2[1, 1]
             x, y = A0[:, p].copy(), A0[:, q].copy()
             x[q] = 0.0
             y[p] = 0.0
-            nx, ny, g = float(x @ x), float(y @ y), float(x @ y)
-            c1 = (1.0 - z11) * (1.0 + z11) - z12 * z12
-            c2 = (1.0 - z22) * (1.0 + z22) - z21 * z21
-            c3 = z11 * z21 + z12 * z22
-            w = d + (nx * c1 + ny * c2 - 2.0 * c3 * g)
+            if cplx:
+                d = 0.0
+                for u, v in ((aqp.real, a1.real), (aqp.imag, a1.imag), (apq.real, a2.real), (apq.imag, a2.imag)):
+                    d += (u - v) * (u + v)
+                nx, ny = float(np.vdot(x, x).real), float(np.vdot(y, y).real)
+                g = complex(np.vdot(x, y))
+                c1 = (1.0 - z11.real) * (1.0 + z11.real) - z11.imag ** 2 - abs(z12) ** 2
+                c2 = (1.0 - z22.real) * (1.0 + z22.real) - z22.imag ** 2 - abs(z21) ** 2
+                c3 = np.conj(z11) * z21 + np.conj(z12) * z22
+                w = d + (nx * c1 + ny * c2 - 2.0 * (c3 * g).real)
+            else:
+                d = (aqp - a1) * (aqp + a1) + (apq - a2) * (apq + a2)
+                nx, ny, g = float(x @ x), float(y @ y), float(x @ y)
+                c1 = (1.0 - z11) * (1.0 + z11) - z12 * z12
+                c2 = (1.0 - z22) * (1.0 + z22) - z21 * z21
+                c3 = z11 * z21 + z12 * z22
+                w = d + (nx * c1 + ny * c2 - 2.0 * c3 * g)
             Wg[k] = w
-            X[k] = bf16([_lg64(w), -1.0 if w < 0 else 1.0, _lg64(nx), _lg64(ny), _lg64(g), _lg64(d),
+            X[k] = bf16([_lg64(w), -1.0 if w < 0 else 1.0, _lg64(nx), _lg64(ny), _lg64(abs(g)), _lg64(d),
                          _lg64(abs(z12) + abs(z21)), min(np.float32(step) / np.float32(10.0 * n), np.float32(4.0))])
     return X.astype(np.float32), Wg
 

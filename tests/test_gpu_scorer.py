@@ -40,9 +40,17 @@ def _dev(torch, dev, Y):
     return torch.from_numpy(np.ascontiguousarray(np.asarray(Y).T)).to(dev).t()
 
 
-def test_gram_features_match_oracle():
+@pytest.mark.parametrize("case", ["real", "complex"])
+def test_gram_features_match_oracle(case):
     torch, jk, scorer, dev = _env()
-    Y, J = gen.graded(40, 1e-3, seed=5)
+    if case == "real":
+        Y, J = gen.graded(40, 1e-3, seed=5)
+    else:
+        # odd order (a partial last chunk of the Gram product), J in a seeded permutation
+        # (pairs whose "-" column comes first take the conjugate product)
+        Y, J = gen.complex_gaussian(41, seed=5, n_plus=23)
+        J = J[np.random.default_rng(5).permutation(41)]
+        Y[:, 4] *= 1e-3
     Y[3, 7] = 0.0
     X, Wg, plus, minus = scorer.features(_dev(torch, dev, Y), J, 17)
     Xn, Wn = om.features(Y, J, 17)
@@ -96,8 +104,8 @@ def _solve(torch, dev, Y, J, sc=None, n_2=0):
     import jkogb_b200 as jk
     n = Y.shape[0]
     A = _dev(torch, dev, Y).clone()
-    U = torch.empty((n, n), dtype=torch.float64, device=dev).t()
-    Z = torch.empty((n, n), dtype=torch.float64, device=dev).t()
+    U = torch.empty((n, n), dtype=A.dtype, device=dev).t()
+    Z = torch.empty((n, n), dtype=A.dtype, device=dev).t()
     s = torch.empty(n, dtype=torch.float64, device=dev)
     torch.cuda.synchronize(dev)
     t0 = time.perf_counter()
@@ -161,3 +169,35 @@ def test_learned_beats_plain_wall_time_at_equal_accuracy():
     R = learned["U"] @ np.diag(learned["sigma"]) @ learned["Z"] - Y
     assert np.linalg.norm(R) <= 1e-12 * np.linalg.norm(Y)
     assert learned["seconds"] < plain["seconds"], (learned["seconds"], plain["seconds"])
+
+
+def test_complex_scored_solves_accurate():
+    """The scored ranking of complex matrices (jk_zstep_loop_dev_scored): the Gram form
+    (Re and Im of x^H y from one FP64 matrix product over interleaved columns) and the
+    trained network against the exact complex weights, through the solve's results (the
+    bounds of test_scored_solves_accurate_and_trained_beats_untrained); the Gram form takes
+    the exact method's number of steps within 5%."""
+    torch, jk, scorer, dev = _env()
+    gram = scorer.Scorer(None, stall_k=8)
+    trained = scorer.Scorer(scorer.load_params(), stall_k=8)
+    steps = {"exact": 0, "gram": 0, "trained": 0}
+    Y2, J2 = gen.complex_gaussian(97, seed=312)
+    cases = (gen.complex_gaussian(64, seed=311, n_plus=40), (Y2, J2[np.random.default_rng(312).permutation(97)]))
+    for Y, J in cases:
+        n = Y.shape[0]
+        Y = np.asarray(Y, np.complex128)
+        ref, _ = oracle.accurate_sigma(Y, J, "q")
+        exact = None
+        for name, sc in (("exact", None), ("gram", gram), ("trained", trained)):
+            r = _solve(torch, dev, Y, J, sc)
+            assert r["info"] > 0, f"{name} n={n}: INFO {r['info']}"
+            assert oracle.sigma_rel_err(r["sigma"], ref, J) <= 1e-12, f"{name} n={n}: sigma"
+            if exact is None:
+                exact = r["sigma"]
+            assert oracle.sigma_rel_err(r["sigma"], exact, J) <= 1e-12, f"{name} n={n}: sigma vs the exact method"
+            R = r["U"] @ np.diag(r["sigma"]) @ r["Z"] - Y
+            assert np.linalg.norm(R) <= 1e-12 * np.linalg.norm(Y), f"{name} n={n}: Y != U SIGMA Z"
+            steps[name] += r["info"]
+    gram.close()
+    trained.close()
+    assert abs(steps["gram"] - steps["exact"]) <= 0.05 * steps["exact"], steps

@@ -1,6 +1,7 @@
 """The learned ranking's host-side pieces that need no GPU: the numpy oracle's BF16
 rounding, gradient and Gram features, and the training target."""
 import numpy as np
+import pytest
 
 import oracle.mlp as om
 
@@ -41,12 +42,15 @@ def test_target_is_the_clamped_log_ratio():
     assert np.allclose(t, [0.0, 1.0, -0.5, 0.8, -1.0, 0.0, 0.0])
 
 
-def test_oracle_gram_form_equals_the_exact_weights():
+@pytest.mark.parametrize("case", ["real", "complex"])
+def test_oracle_gram_form_equals_the_exact_weights(case):
     """w_gram of the numpy oracle against the C oracle's exact weights (the same reduction
-    summed in another order): 1e-10 relative on graded input."""
+    summed in another order): 1e-10 relative on graded real input and on complex Gaussian
+    input with an unbalanced J (ZMAGF2H's weights, whose scan sums |.|^2 of complex
+    entries)."""
     import oracle
     from jkogb_b200 import gen
-    Y, J = gen.graded(24, 1e-4, seed=8)
+    Y, J = gen.graded(24, 1e-4, seed=8) if case == "real" else gen.complex_gaussian(27, seed=4, n_plus=17)
     X, Wg = om.features(Y, J, 3)
     w, P, Q, tt = oracle.weights(Y, J, id_tru=1, nt=1)
     ex = {(int(p) - 1, int(q) - 1): v for p, q, v in zip(P, Q, w)}
