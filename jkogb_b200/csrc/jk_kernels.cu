@@ -262,40 +262,102 @@ __device__ __forceinline__ bool hyp_pair_setup(const double *__restrict__ A, int
 #endif
 constexpr int kScanUnroll = JK_SCAN_UNROLL;
 
-// K pairs per thread (slots t, t + 256, ...); FAST: no row of this chunk is a p or q;
-// FULL: the chunk has all SCAN_ROWS rows (a compile-time trip count, no bound test)
-template <int K, bool FAST, bool FULL>
-__device__ __forceinline__ void scan_chunk(const double *const *xs, const double *const *ys, const int *pl, const int *ql,
-                                           const int *fl, const double *r1, const double *r2, const double *m1,
-                                           const double *m2, double *d, int rows_)
+// Two rows (r, r + 1 of the chunk) of K pairs' ABODNDF2 chains.  TEST: some pair of the
+// warp has its row p or q among them, so every pair skips its own p and q; inactive slots
+// accumulate garbage that is never stored (a predicated pair of fmas instead of a select
+// of their result).
+template <int K, bool TEST, bool FULL>
+__device__ __forceinline__ void scan_rows2(const double2 *xv, const double2 *yv, int r, int rows, const int *pl,
+                                           const int *ql, const double *r1, const double *r2, const double *m1,
+                                           const double *m2, double *d)
 {
-  const int rows = FULL ? SCAN_ROWS : rows_;
-#pragma unroll kScanUnroll
-  for (int r = 0; r < rows; r += 2) {
-    double2 xv[K], yv[K];
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    if (!FULL && h == 1 && r + 1 >= rows) break;
 #pragma unroll
     for (int k = 0; k < K; ++k) {
-      xv[k] = *(const double2 *)(xs[k] + r);
-      yv[k] = *(const double2 *)(ys[k] + r);
-    }
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      if (!FULL && h == 1 && r + 1 >= rows) break;
-#pragma unroll
-      for (int k = 0; k < K; ++k) {
-        const double x = h ? xv[k].y : xv[k].x, y = h ? yv[k].y : yv[k].x;
-        const double xx = __dmul_rn(fma(y, r1[k], x), m1[k]);
-        const double yy = __dmul_rn(fma(x, r2[k], y), m2[k]);
-        const double s1 = __dsub_rn(x, xx), a1 = __dadd_rn(x, xx), s2 = __dsub_rn(y, yy), a2 = __dadd_rn(y, yy);
-        if (FAST || ((r + h) != pl[k] && (r + h) != ql[k])) {
-          // inactive slots accumulate garbage that is never stored; a predicated pair of fmas
-          // instead of a select of their result
-          d[k] = fma(s1, a1, d[k]);
-          d[k] = fma(s2, a2, d[k]);
-        }
+      const double x = h ? xv[k].y : xv[k].x, y = h ? yv[k].y : yv[k].x;
+      const double xx = __dmul_rn(fma(y, r1[k], x), m1[k]);
+      const double yy = __dmul_rn(fma(x, r2[k], y), m2[k]);
+      const double s1 = __dsub_rn(x, xx), a1 = __dadd_rn(x, xx), s2 = __dsub_rn(y, yy), a2 = __dadd_rn(y, yy);
+      if (!TEST || ((r + h) != pl[k] && (r + h) != ql[k])) {
+        d[k] = fma(s1, a1, d[k]);
+        d[k] = fma(s2, a2, d[k]);
       }
     }
   }
+}
+
+// rows of a chunk that share one decision whether to run the skip test (a tuning knob)
+#ifndef JK_SCAN_SUB
+#define JK_SCAN_SUB 32
+#endif
+constexpr int kScanSub = JK_SCAN_SUB;
+static_assert(SCAN_ROWS % kScanSub == 0 && kScanSub % 2 == 0, "sub-blocks tile the chunk in row pairs");
+
+// rows r0 .. r0 + kScanSub - 1 of a full chunk
+template <int K, int SHARED, bool TEST>
+__device__ __forceinline__ void scan_sub(const double *const *xs, const double *const *ys, const double *sh, int r0,
+                                         const int *pl, const int *ql, const double *r1, const double *r2,
+                                         const double *m1, const double *m2, double *d)
+{
+#pragma unroll kScanUnroll
+  for (int r = r0; r < r0 + kScanSub; r += 2) {
+    double2 xv[K], yv[K];
+    double2 sv = make_double2(0.0, 0.0);
+    if (SHARED) sv = *(const double2 *)(sh + r);
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      xv[k] = (SHARED == 2) ? sv : *(const double2 *)(xs[k] + r);
+      yv[k] = (SHARED == 1) ? sv : *(const double2 *)(ys[k] + r);
+    }
+    scan_rows2<K, TEST, true>(xv, yv, r, SCAN_ROWS, pl, ql, r1, r2, m1, m2, d);
+  }
+}
+
+// One row chunk of K pairs per thread (slots t, t + 256, ...).  SHARED 0: pair k scans
+// columns xs[k] (its p) and ys[k] (its q); SHARED 1: every pair's q column is `sh` (one
+// load serves all K); SHARED 2: every pair's p column is `sh`.  `touch` (warp-uniform)
+// marks the chunk's rows that are some pair's p or q: only the sub-blocks of kScanSub
+// rows that hold one run the skip test.  FULL: the chunk has all SCAN_ROWS rows; the
+// last, shorter chunk always runs the test.
+template <int K, int SHARED, bool FULL>
+__device__ __forceinline__ void scan_chunk(const double *const *xs, const double *const *ys, const double *sh,
+                                           const int *pl, const int *ql, const double *r1, const double *r2,
+                                           const double *m1, const double *m2, double *d, int rows,
+                                           unsigned long long touch)
+{
+  if constexpr (FULL) {
+#pragma unroll 1
+    for (int r0 = 0; r0 < SCAN_ROWS; r0 += kScanSub) {
+      if ((touch >> r0) & ((2ull << (kScanSub - 1)) - 1ull)) scan_sub<K, SHARED, true>(xs, ys, sh, r0, pl, ql, r1, r2, m1, m2, d);
+      else scan_sub<K, SHARED, false>(xs, ys, sh, r0, pl, ql, r1, r2, m1, m2, d);
+    }
+  }
+  else {
+#pragma unroll 1
+    for (int r = 0; r < rows; r += 2) {
+      double2 xv[K], yv[K];
+#pragma unroll
+      for (int k = 0; k < K; ++k) {
+        xv[k] = *(const double2 *)(xs[k] + r);
+        yv[k] = *(const double2 *)(ys[k] + r);
+      }
+      scan_rows2<K, true, false>(xv, yv, r, rows, pl, ql, r1, r2, m1, m2, d);
+    }
+  }
+}
+
+template <int SHARED, bool FULL>
+__device__ __forceinline__ void scan_chunk_kw(int kw, const double *const *xs, const double *const *ys, const double *sh,
+                                              const int *pl, const int *ql, const double *r1, const double *r2,
+                                              const double *m1, const double *m2, double *d, int rows,
+                                              unsigned long long touch)
+{
+  if (kw == 4) scan_chunk<4, SHARED, FULL>(xs, ys, sh, pl, ql, r1, r2, m1, m2, d, rows, touch);
+  else if (kw == 3) scan_chunk<3, SHARED, FULL>(xs, ys, sh, pl, ql, r1, r2, m1, m2, d, rows, touch);
+  else if (kw == 2) scan_chunk<2, SHARED, FULL>(xs, ys, sh, pl, ql, r1, r2, m1, m2, d, rows, touch);
+  else if (kw == 1) scan_chunk<1, SHARED, FULL>(xs, ys, sh, pl, ql, r1, r2, m1, m2, d, rows, touch);
 }
 
 #define SCAN_THREADS 256
@@ -380,9 +442,23 @@ k_hyp_pm(const State *st, const double *__restrict__ A, const int *__restrict__ 
     if (SCAN_THREADS * k + 32 * warp < cnt) kw = k + 1;
   }
   int any = 0, fastv = 1;
+  // the column layout of this thread's scanned pairs: whether p is the "+" vertex (xp)
+  // and which "-" column they use (mc), if all of them agree (uni)
+  int xp = -1, mc = TW;
+  bool uni = true;
 #pragma unroll
   for (int k = 0; k < K; ++k)
-    if (fl[k] & 1) { any = 1; if ((fl[k] & 6) != 6) fastv = 0; }
+    if (fl[k] & 1) {
+      any = 1;
+      if ((fl[k] & 6) != 6) fastv = 0;
+      const int cx = cpq[k] & 0xFF, cy = (cpq[k] >> 8) & 0xFF, isp = (cx < TW) ? 1 : 0, m = isp ? cy : cx;
+      if (xp < 0) { xp = isp; mc = m; }
+      else if (xp != isp || mc != m) uni = false;
+    }
+  // SHARED 1: every scanned pair of the warp has p = its "+" vertex and one "-" column
+  // per thread, so that column is every pair's q column; SHARED 2: the "-" vertex is p
+  // (with J's signs in a random permutation, only tiles near the diagonal mix the two)
+  const int shared = __all_sync(0xFFFFFFFFu, uni && xp != 0) ? 1 : (__all_sync(0xFFFFFFFFu, uni && xp != 1) ? 2 : 0);
   // (this barrier also ends every read of tpar before the row buffer overwrites it)
   if (!__syncthreads_or(any)) return;
   const bool allfast = __syncthreads_and(fastv);
@@ -414,34 +490,32 @@ k_hyp_pm(const State *st, const double *__restrict__ A, const int *__restrict__ 
     const int i0 = c * SCAN_ROWS, rows = min(SCAN_ROWS, n - i0);
     const double *xs[K], *ys[K];
     int pr[K], qr[K];
-    bool mine = false;
+    unsigned long long mine = 0;  // the chunk's rows that are p or q of this thread's scanned pairs
 #pragma unroll
     for (int k = 0; k < K; ++k) {
       xs[k] = bb + (cpq[k] & 0xFF) * SCAN_RS;
       ys[k] = bb + ((cpq[k] >> 8) & 0xFF) * SCAN_RS;
       pr[k] = pv[k] - i0;  // p, q as rows of this chunk
       qr[k] = qv[k] - i0;
-      if (fl[k] & 1) mine = mine || (pr[k] >= 0 && pr[k] < rows) || (qr[k] >= 0 && qr[k] < rows);
-    }
-    const bool touch = __any_sync(0xFFFFFFFFu, mine);
-    if (allfast) {
-      if (!touch && rows == SCAN_ROWS) {
-        if (kw == 4) scan_chunk<4, true, true>(xs, ys, pr, qr, fl, r1, r2, m1, m2, d, rows);
-        else if (kw == 3) scan_chunk<3, true, true>(xs, ys, pr, qr, fl, r1, r2, m1, m2, d, rows);
-        else if (kw == 2) scan_chunk<2, true, true>(xs, ys, pr, qr, fl, r1, r2, m1, m2, d, rows);
-        else if (kw == 1) scan_chunk<1, true, true>(xs, ys, pr, qr, fl, r1, r2, m1, m2, d, rows);
+      if (fl[k] & 1) {
+        if (pr[k] >= 0 && pr[k] < rows) mine |= 1ull << pr[k];
+        if (qr[k] >= 0 && qr[k] < rows) mine |= 1ull << qr[k];
       }
-      else if (!touch) {
-        if (kw == 4) scan_chunk<4, true, false>(xs, ys, pr, qr, fl, r1, r2, m1, m2, d, rows);
-        else if (kw == 3) scan_chunk<3, true, false>(xs, ys, pr, qr, fl, r1, r2, m1, m2, d, rows);
-        else if (kw == 2) scan_chunk<2, true, false>(xs, ys, pr, qr, fl, r1, r2, m1, m2, d, rows);
-        else if (kw == 1) scan_chunk<1, true, false>(xs, ys, pr, qr, fl, r1, r2, m1, m2, d, rows);
+    }
+    if (allfast) {
+      const unsigned long long touch =
+          (unsigned long long)__reduce_or_sync(0xFFFFFFFFu, (unsigned)mine) |
+          ((unsigned long long)__reduce_or_sync(0xFFFFFFFFu, (unsigned)(mine >> 32)) << 32);
+      const double *sh = bb + mc * SCAN_RS;
+      if (rows == SCAN_ROWS) {
+        if (shared == 1) scan_chunk_kw<1, true>(kw, xs, ys, sh, pr, qr, r1, r2, m1, m2, d, rows, touch);
+        else if (shared == 2) scan_chunk_kw<2, true>(kw, xs, ys, sh, pr, qr, r1, r2, m1, m2, d, rows, touch);
+        else scan_chunk_kw<0, true>(kw, xs, ys, sh, pr, qr, r1, r2, m1, m2, d, rows, touch);
       }
       else {
-        if (kw == 4) scan_chunk<4, false, false>(xs, ys, pr, qr, fl, r1, r2, m1, m2, d, rows);
-        else if (kw == 3) scan_chunk<3, false, false>(xs, ys, pr, qr, fl, r1, r2, m1, m2, d, rows);
-        else if (kw == 2) scan_chunk<2, false, false>(xs, ys, pr, qr, fl, r1, r2, m1, m2, d, rows);
-        else if (kw == 1) scan_chunk<1, false, false>(xs, ys, pr, qr, fl, r1, r2, m1, m2, d, rows);
+        if (shared == 1) scan_chunk_kw<1, false>(kw, xs, ys, sh, pr, qr, r1, r2, m1, m2, d, rows, touch);
+        else if (shared == 2) scan_chunk_kw<2, false>(kw, xs, ys, sh, pr, qr, r1, r2, m1, m2, d, rows, touch);
+        else scan_chunk_kw<0, false>(kw, xs, ys, sh, pr, qr, r1, r2, m1, m2, d, rows, touch);
       }
     }
     else {
