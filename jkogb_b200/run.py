@@ -1,13 +1,15 @@
 """Run one named workload through the library on the current GPU.
 
   python -m jkogb_b200.run WORKLOAD [--max-steps S] [--weights R] [--save-state F] [--load-state F]
+                                    [--ranking exact|gram|learned] [--save-sigma F]
   python -m jkogb_b200.run batch4096 [--matrices M] [--min-n K] [--max-steps S]
 
 Without --weights: one device-resident solve of the workload (jk_solver_*), stopped after S
 steps when --max-steps is given, and prints the steps, INFO and the wall time.  --save-state
 writes the loop's matrix (with its diagonal) where the run stopped to the .npy file F;
 --load-state starts the run from such a matrix instead of the workload's input, so that a
-profiler can look at a stretch deep inside the solve without replaying its start.  --ranking
+profiler can look at a stretch deep inside the solve without replaying its start.  --save-sigma
+writes the solve's SIGMA to the .npy file F.  --ranking
 gram / learned: the scored solve (jk_dstep_loop_dev_scored) with the Gram form alone or with the
 trained network's correction.  With --weights R: R launches of
 one build's pair weights (jk_handle_weights) on the workload's input Y, the kernel-level
@@ -35,6 +37,7 @@ def main(argv=None):
     ap.add_argument("--weights", type=int, default=0)
     ap.add_argument("--save-state", default="")
     ap.add_argument("--load-state", default="")
+    ap.add_argument("--save-sigma", default="")
     ap.add_argument("--ranking", default="exact", choices=["exact", "gram", "learned"])
     a = ap.parse_args(argv)
 
@@ -81,6 +84,8 @@ def main(argv=None):
         info, exact = sc.step_loop_dev(A, U, Z, s, J, n_2=n_2, stream=stream, max_steps=a.max_steps)
         sc.close()
         torch.cuda.synchronize(dev)
+        if a.save_sigma:
+            np.save(a.save_sigma, s.cpu().numpy())
         print(f"{a.workload} ({a.ranking}): INFO={info}, {exact} exact steps in {time.perf_counter() - t0:.3f} s")
         return 0
     sv = jk.Solver(n, J, n_2=n_2, complex_=cplx)
@@ -93,6 +98,8 @@ def main(argv=None):
     info = sv.finish(s.data_ptr())
     sv.close()
     torch.cuda.synchronize(dev)
+    if a.save_sigma:
+        np.save(a.save_sigma, s.cpu().numpy())
     print(f"{a.workload}: {steps} steps, INFO={info} in {time.perf_counter() - t0:.3f} s")
     return 0
 

@@ -32,6 +32,7 @@ CASES = {
     "complex384": (lambda: gen.complex_gaussian(384, seed=3), "q"),
     "djk_n2048_graded": (lambda: gen.graded(2048, 1e-6, seed=2), "ld"),
     "zjk_n1024": (lambda: gen.complex_gaussian(1024, seed=3), "ld"),
+    "djk_n4096_graded": (lambda: gen.WORKLOADS["djk_n4096_graded"]["make"](), "ld"),
 }
 
 

@@ -229,12 +229,21 @@ def test_device_pointer_entry():
     assert _same(U.cpu().numpy(), o["U"]) and _same(s.cpu().numpy(), o["sigma"])
 
 
-@pytest.mark.parametrize("graded", [False, True])
-def test_weights_bitexact_large_tiles(graded):
-    """Orders large enough for the two-kernel real hyperbolic path (setup + pipelined scan)."""
+@pytest.mark.parametrize("case", ["sorted", "graded", "unbalanced"])
+def test_weights_bitexact_large_tiles(case):
+    """Orders large enough for the two-kernel real hyperbolic path (setup + pipelined scan):
+    J sorted (every pair of a warp has its "+" vertex as p: the shared-column scan), J in a
+    seeded permutation (tiles near the diagonal mix the two orientations), and an odd order
+    with 700 "+" signs in a permutation (partial tiles in both directions, warps with fewer
+    than four pairs per thread)."""
     jk = _jk()
-    n = 800
-    Y, J = gen.graded(n, 1e-6, seed=21) if graded else gen.gaussian(n, seed=21, n_plus=400)
+    if case == "sorted":
+        Y, J = gen.gaussian(800, seed=21, n_plus=400)
+    elif case == "graded":
+        Y, J = gen.graded(800, 1e-6, seed=21)
+    else:
+        Y, J = gen.gaussian(1811, seed=9, n_plus=700)
+        J = J[np.random.default_rng(5).permutation(1811)]
     W = jk.weights(Y, J)
     w, P, Q, tt = oracle.weights(Y, J, id_tru=1, nt=8)
     got = W[P - 1, Q - 1]
