@@ -668,6 +668,246 @@ k_weights_hyp_z(const State *st, const double2 *__restrict__ A, const double *__
   }
 }
 
+// The complex hyperbolic weights, pipelined (k_hyp_z_pm below): sign-class tiles of 16
+// "+" by 32 "-" vertices (512 pairs, two per thread), 32 rows per chunk of the columns
+// and of their unrotated magnitudes staged with cp.async in two buffers, the sequential
+// ABODNZF2 chains of the two pairs of a thread interleaved.
+#define ZTP 16
+#define ZTM 32
+#define ZTC (ZTP + ZTM)
+#define ZROWS 32
+#define ZRS (ZROWS + 1)  // padded column: the 16-byte (8-byte) reads of a warp hit distinct banks
+#define ZSTAGES 2
+#define ZTHREADS 256
+constexpr size_t kZStage = (size_t)ZTC * ZRS * (sizeof(double2) + sizeof(double));
+constexpr size_t kZSmem = ZSTAGES * kZStage;
+
+// scan parameters of one complex hyperbolic pair
+struct ZHypPar {
+  double2 r1, r2, m1, m2;  // the AB coefficients of Z2
+  double d;                // the four leading terms
+  int p, q;                // the pair (0-based, p < q)
+  int flags;               // bit0 scan, bit1 c1, bit2 c2
+  int cols;                // the tile columns of p (bits 0-7) and q (bits 8-15)
+};
+static_assert(ZTP * ZTM * sizeof(ZHypPar) <= kZSmem, "a tile's scan parameters must fit in the row buffer");
+
+// hypot2 out of line: the rare operands hypot2_fast does not take
+__device__ __noinline__ double hypot2_call(double x, double y) { return hypot2(x, y); }
+
+__device__ __forceinline__ double zabs_scan(double2 a)
+{
+  const double ax = fabs(a.x), ay = fabs(a.y);
+  const double u = (ax >= ay) ? ax : ay;
+  const double v = (ax >= ay) ? ay : ax;
+  const int bu = (int)((unsigned long long)__double_as_longlong(u) >> 52);
+  const int bv = (int)((unsigned long long)__double_as_longlong(v) >> 52);
+  if (bu >= 23 && bu <= 2021 && bv >= 1 && ax == ax && ay == ay) return hypot2_fast(a.x, a.y);
+  return hypot2_call(a.x, a.y);
+}
+
+// rows 0 .. rows - 1 of a chunk for K pairs per thread (ABODNZF2, src/Z/ztransf.F90:452-637:
+// the rotation, then the magnitudes of the rotated and of the unrotated entries, rows p and
+// q skipped).  FAST: every pair of the block takes the first branch (c1, c2); otherwise
+// each pair selects its branches.  Slots without a scan compute nothing.
+template <int K, bool FAST>
+__device__ __forceinline__ void zscan_rows(const double2 *const *xs, const double2 *const *ys, const double *const *xa,
+                                           const double *const *ya, int rows, const int *pl, const int *ql,
+                                           const int *fl, const ZRot *t, double *d)
+{
+#pragma unroll 1
+  for (int r = 0; r < rows; ++r) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      if (!(fl[k] & 1)) continue;
+      double2 x = xs[k][r], y = ys[k][r];
+      if (FAST) {
+        const double2 xx = zzfma(y, t[k].r1, x), yy = zzfma(x, t[k].r2, y);
+        x = zzmul(xx, t[k].m1);
+        y = zzmul(yy, t[k].m2);
+      }
+      else zrot_apply_ab(t[k], x, y);
+      if (r != pl[k] && r != ql[k]) {
+        const double axi = xa[k][r], axx = zabs_scan(x), ayi = ya[k][r], ayy = zabs_scan(y);
+        d[k] = fma(__dsub_rn(axi, axx), __dadd_rn(axi, axx), d[k]);
+        d[k] = fma(__dsub_rn(ayi, ayy), __dadd_rn(ayi, ayy), d[k]);
+      }
+    }
+  }
+}
+
+// one complex sign-class tile: tile t holds the pairs of the "+" vertices plus[16 (t / TM) ..]
+// with the "-" vertices minus[32 (t % TM) ..] (TM tiles of "-" vertices), all hyperbolic.
+// First the 2x2 HSVDs of ZMAGF2H (src/Z/zstep.F90:43-74; the scan parameters of the pairs
+// that need the column scan, compacted into the shared memory the row buffer takes over
+// once every thread holds its own pairs' parameters; the other weights straight to W), then
+// the tile's 48 columns and their magnitudes stream through two buffers in row chunks.
+__global__ void __launch_bounds__(ZTHREADS, 2)
+k_hyp_z_pm(const State *st, const double2 *__restrict__ A, const double *__restrict__ mag, const int *__restrict__ plus,
+           const int *__restrict__ minus, int n_plus, int n_minus, int n, double *__restrict__ Wm)
+{
+  if (st->stop || st->learned_step) return;  // a learned step ranks these pairs by the scorer
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int TM = (n_minus + ZTM - 1) / ZTM;
+  const int P0 = (blockIdx.x / TM) * ZTP, Q0 = (blockIdx.x % TM) * ZTM;
+  ZHypPar *tpar = (ZHypPar *)smem_raw;  // [ZTP * ZTM], before the row buffer takes the space
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  __shared__ int s_cnt, s_warp[ZTHREADS / 32], s_col[ZTC];
+  if (tid < ZTC) {
+    const int c = tid;
+    s_col[c] = (c < ZTP) ? ((P0 + c < n_plus) ? plus[P0 + c] : -1) : ((Q0 + c - ZTP < n_minus) ? minus[Q0 + c - ZTP] : -1);
+  }
+  if (tid == 0) s_cnt = 0;
+  __syncthreads();
+  for (int base = 0; base < ZTP * ZTM; base += ZTHREADS) {
+    const int l = base + tid;
+    const int ci = l / ZTM, cj = ZTP + l % ZTM;  // tile columns of the "+" and the "-" vertex
+    const int a = s_col[ci], b = s_col[cj];
+    const bool valid = (a >= 0) && (b >= 0);
+    const unsigned m = __ballot_sync(0xFFFFFFFFu, valid);
+    if (!lane) s_warp[warp] = __popc(m);
+    __syncthreads();
+    int off = s_cnt;
+    for (int w2 = 0; w2 < warp; ++w2) off += s_warp[w2];
+    const int slot = off + __popc(m & ((1u << lane) - 1u));
+    __syncthreads();
+    if (tid == 0) { int t = 0; for (int w2 = 0; w2 < ZTHREADS / 32; ++w2) t += s_warp[w2]; s_cnt += t; }
+    if (valid) {
+      const bool ap = (a < b);
+      const int p = ap ? a : b, q = ap ? b : a;
+      const double2 app = A[(long long)p * n + p], aqp = A[(long long)p * n + q], apq = A[(long long)q * n + p],
+                    aqq = A[(long long)q * n + q];
+      ZHypPar h;
+      h.p = p; h.q = q;
+      h.cols = ap ? (ci | (cj << 8)) : (cj | (ci << 8));
+      h.flags = 0;
+      h.d = 0.0;
+      h.r1 = h.r2 = h.m1 = h.m2 = make_double2(0.0, 0.0);
+      double w = nan_w();
+      if (may_transform(app, aqp, apq, aqq)) {
+        double2 A2[4] = { app, aqp, apq, aqq }, U2[4], Z2[4];
+        int info = 0;
+        const int jp = ap ? 1 : -1;  // "+" column a, "-" column b
+        zhsvd2(A2, jp, -jp, U2, Z2, JK_TH1FIX, info);
+        if (info < 0) w = nan_w();
+        else if (!(info & 1)) w = 0.0;
+        else if (!(info & 4)) w = dasum4(aqp.x, aqp.y, apq.x, apq.y);
+        else {
+          // the four off-diagonal terms that start ABODNZF2
+          const double2 a1 = (info & 8) ? A2[M21] : make_double2(0.0, 0.0);
+          const double2 a2 = (info & 8) ? A2[M12] : make_double2(0.0, 0.0);
+          double d = 0.0;
+          d = fma(__dsub_rn(aqp.x, a1.x), __dadd_rn(aqp.x, a1.x), d);
+          d = fma(__dsub_rn(aqp.y, a1.y), __dadd_rn(aqp.y, a1.y), d);
+          d = fma(__dsub_rn(apq.x, a2.x), __dadd_rn(apq.x, a2.x), d);
+          d = fma(__dsub_rn(apq.y, a2.y), __dadd_rn(apq.y, a2.y), d);
+          const ZRot t = zrot_ab(Z2);
+          h.r1 = t.r1; h.r2 = t.r2; h.m1 = t.m1; h.m2 = t.m2;
+          h.flags = 1 | (t.c1 ? 2 : 0) | (t.c2 ? 4 : 0);
+          h.d = d;
+        }
+      }
+      tpar[slot] = h;
+      if (!(h.flags & 1)) {
+        if (w < -JK_HUGE) w = nan_w();
+        Wm[(long long)q * n + p] = w;
+        Wm[(long long)p * n + q] = w;
+      }
+    }
+    __syncthreads();
+  }
+  const int cnt = s_cnt;
+  if (!cnt) return;
+
+  double2 *bz = (double2 *)smem_raw;                                          // [ZSTAGES][ZTC][ZRS]
+  double *bm = (double *)(smem_raw + ZSTAGES * ZTC * ZRS * sizeof(double2));  // [ZSTAGES][ZTC][ZRS]
+  constexpr int K = 2, STAGE = ZTC * ZRS;
+  int pv[K], qv[K], cpq[K], fl[K];
+  ZRot t[K];
+  double d[K];
+  int kw = 0;  // active slots of this warp (warp-uniform)
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    const int slot = tid + ZTHREADS * k;
+    fl[k] = 0; pv[k] = qv[k] = -1; cpq[k] = 0; d[k] = 0.0;
+    t[k].r1 = t[k].r2 = t[k].m1 = t[k].m2 = make_double2(0.0, 0.0);
+    t[k].c1 = t[k].c2 = 1;
+    if (slot < cnt) {
+      const ZHypPar h = tpar[slot];
+      fl[k] = h.flags; pv[k] = h.p; qv[k] = h.q; cpq[k] = h.cols; d[k] = h.d;
+      t[k].r1 = h.r1; t[k].r2 = h.r2; t[k].m1 = h.m1; t[k].m2 = h.m2;
+      t[k].c1 = (h.flags >> 1) & 1; t[k].c2 = (h.flags >> 2) & 1;
+    }
+    if (ZTHREADS * k + 32 * warp < cnt) kw = k + 1;
+  }
+  int any = 0, fastv = 1;
+#pragma unroll
+  for (int k = 0; k < K; ++k)
+    if (fl[k] & 1) { any = 1; if ((fl[k] & 6) != 6) fastv = 0; }
+  // (this barrier also ends every read of tpar before the row buffer overwrites it)
+  if (!__syncthreads_or(any)) return;
+  const bool allfast = __syncthreads_and(fastv);
+  const int nchunk = (n + ZROWS - 1) / ZROWS;
+  auto stage = [&](int c) {
+    if (c < nchunk) {
+      double2 *dz = bz + (c % ZSTAGES) * STAGE;
+      double *dm = bm + (c % ZSTAGES) * STAGE;
+      const int i0 = c * ZROWS;
+#pragma unroll
+      for (int j = 0; j < (ZTC * ZROWS) / ZTHREADS; ++j) {
+        const int idx = tid + ZTHREADS * j, col = idx / ZROWS, r = idx % ZROWS;
+        const int g = s_col[col];
+        if (g >= 0 && i0 + r < n) {
+          const long long e = (long long)g * n + i0 + r;
+          cp_async16(dz + col * ZRS + r, A + e);
+          cp_async8(dm + col * ZRS + r, mag + e);
+        }
+      }
+    }
+    cp_async_commit();  // an empty group past the last chunk keeps the wait count uniform
+  };
+  static_assert((ZTC * ZROWS) % ZTHREADS == 0, "the staging copies divide among the threads");
+  stage(0);
+  for (int c = 0; c < nchunk; ++c) {
+    stage(c + 1);        // into the buffer of chunk c - 1, which every thread is done with
+    cp_async_wait<1>();  // chunk c has landed (chunk c + 1 may be in flight)
+    __syncthreads();
+    const double2 *cz = bz + (c % ZSTAGES) * STAGE;
+    const double *cm = bm + (c % ZSTAGES) * STAGE;
+    const int i0 = c * ZROWS, rows = min(ZROWS, n - i0);
+    const double2 *xs[K], *ys[K];
+    const double *xa[K], *ya[K];
+    int pr[K], qr[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const int cx = cpq[k] & 0xFF, cy = (cpq[k] >> 8) & 0xFF;
+      xs[k] = cz + cx * ZRS; ys[k] = cz + cy * ZRS;
+      xa[k] = cm + cx * ZRS; ya[k] = cm + cy * ZRS;
+      pr[k] = pv[k] - i0;  // p, q as rows of this chunk
+      qr[k] = qv[k] - i0;
+    }
+    if (allfast) {
+      if (kw == 2) zscan_rows<2, true>(xs, ys, xa, ya, rows, pr, qr, fl, t, d);
+      else if (kw == 1) zscan_rows<1, true>(xs, ys, xa, ya, rows, pr, qr, fl, t, d);
+    }
+    else {
+      if (kw == 2) zscan_rows<2, false>(xs, ys, xa, ya, rows, pr, qr, fl, t, d);
+      else if (kw == 1) zscan_rows<1, false>(xs, ys, xa, ya, rows, pr, qr, fl, t, d);
+    }
+    __syncthreads();  // every thread is done with chunk c before chunk c + 2 overwrites it
+  }
+  cp_async_wait<0>();
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    if (!(fl[k] & 1)) continue;
+    const int p = pv[k], q = qv[k];
+    double x = d[k];
+    if (x < -JK_HUGE) x = nan_w();
+    Wm[(long long)q * n + p] = x;
+    Wm[(long long)p * n + q] = x;
+  }
+}
+
 template <typename T, int HP, int HM>
 __global__ void __launch_bounds__(HP * HM)
 k_weights_hyp(const State *st, const T *__restrict__ A, const int *__restrict__ plus, const int *__restrict__ minus,
@@ -1711,6 +1951,7 @@ cudaError_t prepare_kernels(int n)
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k_hyp_pm, cudaFuncAttributeMaxDynamicSharedMemorySize, SCAN_STAGES * (2 * TW) * SCAN_RS * (int)sizeof(double));
   if (e == cudaSuccess) e = cudaFuncSetAttribute(k_rotate<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 2 * n * 16);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_hyp_z_pm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kZSmem);
   const int ss = (int)select_smem(n);
   if (e == cudaSuccess) e = cudaFuncSetAttribute(k_select<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, ss);
   if (e == cudaSuccess) e = cudaFuncSetAttribute(k_select<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, ss);
@@ -1785,7 +2026,13 @@ static cudaError_t weights_t(Workspace &w, const T *A, cudaStream_t s)
       const long long nn = (long long)n * n;
       k_absmat<<<(unsigned)((nn + 255) / 256 < 4096 ? (nn + 255) / 256 : 4096), 256, 0, s>>>(w.st, (const double2 *)A, nn,
                                                                                               w.mag);
-      if ((long long)w.n_plus * w.n_minus >= 256LL * 148 * 4) {
+      if ((long long)w.n_plus * w.n_minus >= (long long)ZTP * ZTM * 148) {
+        // the pipelined tiles once they fill the GPU
+        const int nt = ((w.n_plus + ZTP - 1) / ZTP) * ((w.n_minus + ZTM - 1) / ZTM);
+        k_hyp_z_pm<<<nt, ZTHREADS, kZSmem, s>>>(w.st, (const double2 *)A, w.mag, w.plus, w.minus, w.n_plus, w.n_minus, n,
+                                                w.Wm);
+      }
+      else if ((long long)w.n_plus * w.n_minus >= 256LL * 148 * 4) {
         dim3 gh((w.n_plus + 15) / 16, (w.n_minus + 15) / 16);
         k_weights_hyp_z<16, 16><<<gh, 256, 0, s>>>(w.st, (const double2 *)A, w.mag, w.plus, w.minus, w.n_plus, w.n_minus,
                                                   w.Wm, n);

@@ -91,6 +91,35 @@ __device__ __forceinline__ double hypot2(double x, double y)
   return scale(h, ea);
 }
 
+// hypot2 with the power-of-two scalings done by multiplication where that is exact: for
+// finite x, y whose larger magnitude a is normal with exponent in [-999, 999] and whose
+// smaller one b is normal, a * 2^-ea, b * 2^-ea and h * 2^ea are normal numbers (or, for
+// the last, h * 2^ea is rounded once, as SCALE rounds), so every value equals hypot2's bit
+// for bit; everything else goes through hypot2.  The same operations in the same order.
+__device__ __forceinline__ double hypot2_fast(double x, double y)
+{
+  const double ax = fabs(x), ay = fabs(y);
+  const double a = (ax >= ay) ? ax : ay;
+  const double b = (ax >= ay) ? ay : ax;
+  const int ba = (int)((unsigned long long)__double_as_longlong(a) >> 52);
+  const int bb = (int)((unsigned long long)__double_as_longlong(b) >> 52);
+  if (ba >= 23 && ba <= 2021 && bb >= 1 && ax == ax && ay == ay) {
+    const int ea = ba - 1022;
+    if (ea - (bb - 1022) > 54) return a;
+    const double f = __longlong_as_double((long long)(1023 - ea) << 52);
+    const double g = __longlong_as_double((long long)(1023 + ea) << 52);
+    const double as = __dmul_rn(a, f), bs = __dmul_rn(b, f);
+    double h = sqrt(fma(as, as, __dmul_rn(bs, bs)));
+    const double hh = __dmul_rn(h, h), he = fma(h, h, -hh);
+    const double aa = __dmul_rn(as, as), ae = fma(as, as, -aa);
+    const double bq = __dmul_rn(bs, bs), be = fma(bs, bs, -bq);
+    const double r = __dadd_rn(__dadd_rn(__dsub_rn(aa, hh), bq), __dsub_rn(__dadd_rn(ae, be), he));
+    h = __dadd_rn(h, __ddiv_rn(r, __dadd_rn(h, h)));
+    return __dmul_rn(h, g);
+  }
+  return hypot2(x, y);
+}
+
 // QUIET_NAN, src/shared/utils.F90:144-149
 __device__ __forceinline__ double quiet_nan(long long payload)
 {
@@ -440,6 +469,7 @@ __device__ __forceinline__ double2 zneg(double2 a) { return make_double2(-a.x, -
 __device__ __forceinline__ bool zeq0(double2 a) { return (a.x == 0.0) && (a.y == 0.0); }
 __device__ __forceinline__ bool zne1(double2 a) { return (a.x != 1.0) || (a.y != 0.0); }
 __device__ __forceinline__ double zabs(double2 a) { return hypot2(a.x, a.y); }
+__device__ __forceinline__ double zabs_fast(double2 a) { return hypot2_fast(a.x, a.y); }
 
 // ZDFMA, src/Z/ztransf.F90:130-141
 __device__ __forceinline__ double2 zdfma(double a, double2 b, double2 c) { return zc(fma(a, b.x, c.x), fma(a, b.y, c.y)); }

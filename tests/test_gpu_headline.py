@@ -59,8 +59,8 @@ def test_headline_prefix_bitexact(name, make, n_2, k):
 
 def test_complex_weights_n1024_bitexact():
     """The complex weights at the complex workload's order, through k_absmat and the
-    tiled k_weights_hyp_z (the production path at N = 1024), on the input and after a
-    few steps."""
+    pipelined sign-class tiles of k_hyp_z_pm (the production path at N = 1024), on the
+    input and after a few steps."""
     jk = _jk()
     Y, J = gen.complex_gaussian(1024, seed=3)
     A = jk.step_loop(Y, J, n_2=512, max_steps=2)["A"]
@@ -71,3 +71,20 @@ def test_complex_weights_n1024_bitexact():
         assert np.array_equal(np.isnan(got), np.isnan(w))
         m = ~np.isnan(w)
         assert _same(got[m], w[m])
+
+
+def test_complex_weights_partial_tiles_bitexact():
+    """The pipelined complex tiles with partial tiles in both directions and both pair
+    orientations: N = 700 with 300 "+" signs in a seeded permutation, and a column scaled
+    down so that rotated entries leave the range of the multiplication-scaled hypot."""
+    jk = _jk()
+    Y, J = gen.complex_gaussian(700, seed=4, n_plus=300)
+    J = J[np.random.default_rng(6).permutation(700)]
+    Y[:, 5] *= 1e-305
+    Y[:, 9] *= 1e300
+    W = jk.weights(Y, J)
+    w, P, Q, tt = oracle.weights(Y, J, id_tru=1, nt=NT)
+    got = W[P - 1, Q - 1]
+    assert np.array_equal(np.isnan(got), np.isnan(w))
+    m = ~np.isnan(w)
+    assert _same(got[m], w[m])
