@@ -39,6 +39,8 @@ def lib():
         L.jo_zstep_loop.argtypes = [C.c_int, dp, C.c_int, dp, C.c_int, dp, C.c_int, ip, dp,
                                     C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p]
         L.jo_dhsvd2.argtypes = [dp, ip, dp, dp, C.c_double, ip]
+        L.jo_hypot_identity_check.restype = C.c_longlong
+        L.jo_hypot_identity_check.argtypes = [C.c_longlong, C.c_ulonglong]
         L.jo_zhsvd2.argtypes = [dp, ip, dp, dp, C.c_double, ip]
         L.jo_dweights.restype = C.c_int
         L.jo_dweights.argtypes = [C.c_int, dp, C.c_int, ip, C.c_int, C.c_int, dp, ip, ip]

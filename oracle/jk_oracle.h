@@ -53,6 +53,10 @@ double jo_quiet_nan(int64_t payload);
 int    jo_exponent(double x);
 double jo_scale(double x, int e);
 double jo_hypot(double x, double y);
+/* the multiplication-scaled form of jo_hypot that the GPU's complex column scan uses, and
+ * the count of seeded operand pairs on which the two differ (jk_hypot_check.c) */
+double jo_hypot_mulscaled(double x, double y);
+long long jo_hypot_identity_check(long long n, unsigned long long seed);
 double jo_dasum2(double x1, double x2);
 double jo_dasum4(double x1, double x2, double x3, double x4);
 
