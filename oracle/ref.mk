@@ -3,7 +3,9 @@
 # oracle tests use as pins.  The Fortran production path cannot be built here
 # (no Fortran compiler; the external libpvn build include is absent).
 #   libjkref_alt.so : src/alt/wpqb.c (record comparator + greedy selection, qsort
-#                     build without OpenMP) and src/alt/j2apq.c (row-cyclic pairs)
+#                     build without OpenMP), src/alt/j2apq.c (row-cyclic pairs) and
+#                     src/alt/tweight.c (extended-precision trigonometric pair weight, with
+#                     the project's plain-double entry points of ref_tw.c)
 #   libjkref_var.so : src/var/qtransf.c, src/var/xtransf.c (80-bit 2x2 HSVDs)
 # wpqb.c keeps its selection count in the padding bytes of an 80-bit long double
 # (a union) and then stores to the long double; an optimising build may drop the
@@ -17,7 +19,7 @@ CFLAGS := -std=gnu18 -fno-strict-aliasing -fPIC -shared -D_GNU_SOURCE -w
 
 all: $(OUT)/libjkref_alt.so $(OUT)/libjkref_var.so
 
-$(OUT)/libjkref_alt.so: $(REF)/src/alt/wpqb.c $(REF)/src/alt/j2apq.c $(REF)/src/alt/common.c
+$(OUT)/libjkref_alt.so: $(REF)/src/alt/wpqb.c $(REF)/src/alt/j2apq.c $(REF)/src/alt/tweight.c $(REF)/src/alt/common.c ref_tw.c
 	mkdir -p $(OUT)
 	$(CC) $(CFLAGS) -O0 -I$(REF)/src/alt -o $@ $^ -lm
 

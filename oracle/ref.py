@@ -4,6 +4,8 @@
   apq_pairs(...)    -- src/alt/j2apq.c:3-52 (row-cyclic pair list, trigonometric first)
   ref_dhsvd2(...)   -- src/var/qtransf.c:322 (80-bit 2x2 HSVD)
   ref_zhsvd2(...)   -- src/var/xtransf.c:426 (80-bit complex 2x2 HSVD)
+  ref_dtw(...), ref_ztw(...) -- src/alt/tweight.c:82-92 (extended-precision trigonometric
+                       pair weight, rounded to double; NaN when it is zero)
 
 The libraries exist only where the reference checkout was present at build time;
 available() says whether they can be used.
@@ -52,7 +54,21 @@ def _alt():
     L.apq_create.argtypes = [C.c_uint16, C.c_void_p]
     L.apq_free.argtypes = [C.POINTER(_Apq)]
     L.apq_free.restype = C.c_void_p
+    L.jkref_dtw.restype = C.c_double
+    L.jkref_dtw.argtypes = [C.c_double, C.c_double]
+    L.jkref_ztw.restype = C.c_double
+    L.jkref_ztw.argtypes = [C.c_double] * 4
     return L
+
+
+def ref_dtw(aqp: float, apq: float) -> float:
+    """src/alt/tweight.c dtw: aqp^2 + apq^2 in extended precision (NaN if 0), rounded to double."""
+    return _alt().jkref_dtw(float(aqp), float(apq))
+
+
+def ref_ztw(aqp: complex, apq: complex) -> float:
+    """src/alt/tweight.c ztw: |aqp|^2 + |apq|^2 in extended precision (NaN if 0), rounded to double."""
+    return _alt().jkref_ztw(aqp.real, aqp.imag, apq.real, apq.imag)
 
 
 def wpqb_select(n: int, w: np.ndarray, P: np.ndarray, Q: np.ndarray, n_s: int) -> np.ndarray:

@@ -8,7 +8,8 @@ src/var/qtransf.c and src/var/xtransf.c through oracle/ref.mk):
 The fixture holds, for seeded inputs, the reference C outputs of
   * the greedy non-colliding selection (src/alt/wpqb.c:196-223),
   * the row-cyclic pair list with trigonometric pairs first (src/alt/j2apq.c:3-52),
-  * the 80-bit real and complex 2x2 HSVDs (src/var/qtransf.c:322, src/var/xtransf.c:426).
+  * the 80-bit real and complex 2x2 HSVDs (src/var/qtransf.c:322, src/var/xtransf.c:426),
+  * the extended-precision trigonometric pair weight (src/alt/tweight.c:82-92).
 """
 import os
 import sys
@@ -77,6 +78,21 @@ def main():
         out[f"{kind}2_j"] = np.array(Js, np.int32)
         out[f"{kind}2_s"] = np.array(S)
         out[f"{kind}2_info"] = np.array(I, np.int32)
+    # trigonometric pair weights: a_qp, a_pq over wide exponent ranges, with zeros (a separate
+    # generator, so that the cases above keep their values)
+    rt = np.random.Generator(np.random.PCG64(20261204))
+    for kind in ("d", "z"):
+        m = 3000
+        X = rt.standard_normal((m, 2)) * np.exp(rt.uniform(-300, 300, (m, 2)))
+        if kind == "z":
+            X = X + 1j * rt.standard_normal((m, 2)) * np.exp(rt.uniform(-300, 300, (m, 2)))
+            X[::11, 0] = X[::11, 0].real  # purely real entries
+        X[::7, 0] = 0.0
+        X[::13, 1] = 0.0
+        X[::91, :] = 0.0  # both zero: no transformation
+        f = ref.ref_ztw if kind == "z" else ref.ref_dtw
+        out[f"tw{kind}_x"] = X
+        out[f"tw{kind}_w"] = np.array([f(a, b) for a, b in X])
     path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "ref_pins.npz")
     np.savez_compressed(path, **out)
     print("wrote", path, os.path.getsize(path), "bytes")

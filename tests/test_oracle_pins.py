@@ -146,3 +146,34 @@ def test_ncp3_takes_the_best_walk():
     for a, b in p3:
         assert a not in used and b not in used
         used |= {int(a), int(b)}
+
+
+def test_trig_weight_against_reference_extended(golden):
+    """DASUM2 / DASUM4 of the oracle (the trigonometric pair weight of DMAGF2T / ZMAGF2T,
+    src/D/dtransf.F90:12-38, src/Z/ztransf.F90:18-75) against the reference's own
+    extended-precision statement of that weight, src/alt/tweight.c:82-92 (dtw, ztw), on
+    seeded entries spanning 1e-130 .. 1e130 with zeros: within two units in the last place
+    (4.5e-16 relative; 98% agree exactly, none differs by more than one unit), and "no
+    transformation" (NaN there, 0 here) exactly when both entries are zero.  The defunct
+    real dfn2 (src/alt/tweight.c:3-22) returns the smaller entry squared, 0, when one entry
+    is zero, so the real comparison excludes the rows with exactly one zero entry."""
+    L = oracle.lib()
+    for kind in ("d", "z"):
+        X, W = golden[f"tw{kind}_x"], golden[f"tw{kind}_w"]
+        n_cmp = 0
+        for (a, b), w in zip(X, W):
+            if kind == "d":
+                got = L.jo_dasum2(float(a.real), float(b.real))
+                zero_a, zero_b = a == 0.0, b == 0.0
+                if zero_a != zero_b:
+                    continue  # the defect above
+            else:
+                got = L.jo_dasum4(float(a.real), float(a.imag), float(b.real), float(b.imag))
+                zero_a = zero_b = (a == 0.0 and b == 0.0)
+            if zero_a and zero_b:
+                assert np.isnan(w) and got == 0.0
+                continue
+            assert np.isfinite(w) and got > 0.0
+            assert abs(got - w) <= 4.5e-16 * w, (kind, a, b, got, w)
+            n_cmp += 1
+        assert n_cmp > 2000
