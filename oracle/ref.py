@@ -6,6 +6,8 @@
   ref_zhsvd2(...)   -- src/var/xtransf.c:426 (80-bit complex 2x2 HSVD)
   ref_dtw(...), ref_ztw(...) -- src/alt/tweight.c:82-92 (extended-precision trigonometric
                        pair weight, rounded to double; NaN when it is zero)
+  ref_hypot_x87(...), ref_dasum2(...), ref_dasum4(...) -- src/var/shared/cutils.c:79-95
+                       (x87 extended-precision HYPOT, DASUM2, DASUM4, rounded to double)
 
 The libraries exist only where the reference checkout was present at build time;
 available() says whether they can be used.
@@ -21,18 +23,19 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _ALT = os.path.join(_HERE, "_ref", "libjkref_alt.so")
 _VAR = os.path.join(_HERE, "_ref", "libjkref_var.so")
+_CUT = os.path.join(_HERE, "_ref", "libjkref_cutils.so")
 # the reference checkout: $JKOGB_REFERENCE, else the repository's sibling directory `reference`
 REF_ROOT = os.environ.get("JKOGB_REFERENCE", os.path.normpath(os.path.join(_HERE, "..", "..", "reference")))
 
 
 def build() -> bool:
-    if not (os.path.exists(_ALT) and os.path.exists(_VAR)):
+    if not (os.path.exists(_ALT) and os.path.exists(_VAR) and os.path.exists(_CUT)):
         if not os.path.isdir(os.path.join(REF_ROOT, "src")):
             return False
         env = dict(os.environ)
         env.pop("CC", None)
         subprocess.run(["make", "-s", "-C", _HERE, "-f", "ref.mk", f"REF={REF_ROOT}"], check=True, env=env)
-    return os.path.exists(_ALT) and os.path.exists(_VAR)
+    return os.path.exists(_ALT) and os.path.exists(_VAR) and os.path.exists(_CUT)
 
 
 def available() -> bool:
@@ -130,3 +133,27 @@ def ref_zhsvd2(A2: np.ndarray, J2) -> tuple[np.ndarray, np.ndarray, np.ndarray, 
     info = np.zeros(1, np.int64)
     _var().zhsvd2_(A.ctypes.data, j.ctypes.data, U.ctypes.data, Z.ctypes.data, info.ctypes.data)
     return A, U, Z, int(info[0])
+
+
+def _cut():
+    L = C.CDLL(_CUT)
+    for nm, k in (("HYPOTwX87", 2), ("DASUM2", 2), ("DASUM4", 4)):
+        f = getattr(L, nm)
+        f.restype = C.c_double
+        f.argtypes = [C.c_double] * k
+    return L
+
+
+def ref_hypot_x87(a: float, b: float) -> float:
+    """src/var/shared/cutils.c HYPOTwX87: sqrt(a^2 + b^2) in x87 extended precision."""
+    return _cut().HYPOTwX87(float(a), float(b))
+
+
+def ref_dasum2(a: float, b: float) -> float:
+    """src/var/shared/cutils.c DASUM2: a^2 + b^2 in x87 extended precision."""
+    return _cut().DASUM2(float(a), float(b))
+
+
+def ref_dasum4(a: float, b: float, c: float, d: float) -> float:
+    """src/var/shared/cutils.c DASUM4: the four squares summed from the smallest, extended precision."""
+    return _cut().DASUM4(float(a), float(b), float(c), float(d))

@@ -9,7 +9,8 @@ The fixture holds, for seeded inputs, the reference C outputs of
   * the greedy non-colliding selection (src/alt/wpqb.c:196-223),
   * the row-cyclic pair list with trigonometric pairs first (src/alt/j2apq.c:3-52),
   * the 80-bit real and complex 2x2 HSVDs (src/var/qtransf.c:322, src/var/xtransf.c:426),
-  * the extended-precision trigonometric pair weight (src/alt/tweight.c:82-92).
+  * the extended-precision trigonometric pair weight (src/alt/tweight.c:82-92),
+  * the x87 extended-precision HYPOT, DASUM2 and DASUM4 (src/var/shared/cutils.c:82-95).
 """
 import os
 import sys
@@ -82,7 +83,7 @@ def main():
     # generator, so that the cases above keep their values)
     rt = np.random.Generator(np.random.PCG64(20261204))
     for kind in ("d", "z"):
-        m = 3000
+        m = 2000
         X = rt.standard_normal((m, 2)) * np.exp(rt.uniform(-300, 300, (m, 2)))
         if kind == "z":
             X = X + 1j * rt.standard_normal((m, 2)) * np.exp(rt.uniform(-300, 300, (m, 2)))
@@ -93,6 +94,19 @@ def main():
         f = ref.ref_ztw if kind == "z" else ref.ref_dtw
         out[f"tw{kind}_x"] = X
         out[f"tw{kind}_w"] = np.array([f(a, b) for a, b in X])
+    # HYPOT, DASUM2, DASUM4 in x87 extended precision: operands over the whole exponent range,
+    # subnormals, zeros, equal magnitudes and wide gaps (again a generator of its own)
+    rh = np.random.Generator(np.random.PCG64(20261205))
+    m = 3000
+    H = rh.standard_normal((m, 4)) * np.exp2(rh.integers(-1070, 1020, (m, 4)).astype(np.float64))
+    H[::5, 1] = H[::5, 0] * rh.uniform(0.5, 2.0, len(H[::5]))  # close magnitudes
+    H[::9, 1] = H[::9, 0] * 2.0 ** -60                             # gaps beyond 54 binades
+    H[::17, 1] = 0.0
+    H[::23, :2] = np.ldexp(rh.uniform(1, 2, (len(H[::23]), 2)), -1060)  # subnormal operands
+    out["hx_x"] = H
+    out["hx_hypot"] = np.array([ref.ref_hypot_x87(a, b) for a, b, _, _ in H])
+    out["hx_dasum2"] = np.array([ref.ref_dasum2(a, b) for a, b, _, _ in H])
+    out["hx_dasum4"] = np.array([ref.ref_dasum4(a, b, c, d) for a, b, c, d in H])
     path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "ref_pins.npz")
     np.savez_compressed(path, **out)
     print("wrote", path, os.path.getsize(path), "bytes")

@@ -176,4 +176,29 @@ def test_trig_weight_against_reference_extended(golden):
             assert np.isfinite(w) and got > 0.0
             assert abs(got - w) <= 4.5e-16 * w, (kind, a, b, got, w)
             n_cmp += 1
-        assert n_cmp > 2000
+        assert n_cmp > 1200
+
+
+def test_hypot_and_dasum_against_reference_x87(golden):
+    """The project-own HYPOT (jo_hypot: exact power-of-two scaling, one Newton step from
+    error-free products; the GPU kernels restate it) against the reference's x87
+    extended-precision HYPOTwX87, and the oracle's DASUM2 / DASUM4 against the extended
+    forms of src/var/shared/cutils.c:82-95, on seeded operands over the whole exponent range
+    (subnormals, zeros, close magnitudes, gaps beyond 54 binades): the hypot bit for bit,
+    DASUM2 / DASUM4 within one unit in the last place (both infinite where the squares
+    overflow)."""
+    L = oracle.lib()
+    H = golden["hx_x"]
+    refs = (("hypot", golden["hx_hypot"], lambda r: L.jo_hypot(r[0], r[1]), 0),
+            ("dasum2", golden["hx_dasum2"], lambda r: L.jo_dasum2(r[0], r[1]), 1),
+            ("dasum4", golden["hx_dasum4"], lambda r: L.jo_dasum4(r[0], r[1], r[2], r[3]), 1))
+    for name, want, f, ulps in refs:
+        n_fin = 0
+        for r, w in zip(H, want):
+            g = f([float(x) for x in r])
+            if not np.isfinite(w):
+                assert g == w, (name, r, g, w)
+                continue
+            assert abs(g - w) <= ulps * np.spacing(abs(w)), (name, r, g, w)
+            n_fin += 1
+        assert n_fin > 1000
