@@ -46,6 +46,9 @@ def _rand_2x2(rng, cnt, cplx):
     B[::29] *= 1e300
     B[::31, 1, 1] = -B[::31, 1, 1]
     J = np.where(rng.uniform(size=(cnt, 2)) < 0.5, 1, -1).astype(np.int32)
+    # equal columns with J = (-1, 1): no hyperbolic transformation, INFO -10 / -11 mostly
+    B[3::37, :, 1] = B[3::37, :, 0]
+    J[3::37] = (-1, 1)
     return B, J
 
 
@@ -57,12 +60,24 @@ def test_hsvd2_batch_bitexact(cplx, th1):
     B, J = _rand_2x2(rng, 3000, cplx)
     B[5] = np.nan
     B[6, 0, 1] = np.inf
+    if not cplx:
+        # blocks whose hyperbolic tangent rounds to 1 or beyond (src/shared/ktransf.F90:76-79, 133-136)
+        h = float.fromhex
+        B[7] = [[h("-0x1.4a1f253355902p+0"), h("-0x1.4a1f253355902p+0")],
+                [h("-0x1.e177757c5cfd8p-3"), h("-0x1.e177757c5cfd8p-3")]]
+        B[8] = [[h("-0x1.66ac4cd29aad3p+0"), h("-0x1.66ac4cd29aad4p+0")],
+                [h("0x1.410e13af8d388p-4"), h("0x1.410e13af8d389p-4")]]
+        J[7] = J[8] = (-1, 1)
     A, U, Z, info = jk.hsvd2_batch(B, J, th1)
+    codes = set()
     for k in range(len(B)):
         a, u, z, inf = oracle.hsvd2(B[k], J[k], th1)
         assert inf == info[k], (k, inf, info[k])
+        codes.add(int(inf))
         if inf >= 0:
             assert _same(a, A[k]) and _same(u, U[k]) and _same(z, Z[k]), k
+    if not cplx:
+        assert {-10, -11} <= codes
 
 
 @pytest.mark.parametrize("cplx", [False, True])

@@ -202,3 +202,30 @@ def test_hypot_and_dasum_against_reference_x87(golden):
             assert abs(g - w) <= ulps * np.spacing(abs(w)), (name, r, g, w)
             n_fin += 1
         assert n_fin > 1000
+
+
+def test_2x2_hyperbolic_tangent_at_one_fails():
+    """A 2x2 block with two (nearly) equal columns and J = diag(-1, 1) has no hyperbolic
+    transformation: KHSVD2U / KHSVD2L find |tanh| >= 1 and return INFO -10 / -11
+    (src/shared/ktransf.F90:76-79, 133-136), which DHSVD2 passes on; the weight phase turns
+    such a pair into "no transformation" (NaN)."""
+    h = float.fromhex
+    cases = [([[h("-0x1.4a1f253355902p+0"), h("-0x1.4a1f253355902p+0")],
+               [h("-0x1.e177757c5cfd8p-3"), h("-0x1.e177757c5cfd8p-3")]], -10),
+             ([[h("-0x1.66ac4cd29aad3p+0"), h("-0x1.66ac4cd29aad4p+0")],
+               [h("0x1.410e13af8d388p-4"), h("0x1.410e13af8d389p-4")]], -11)]
+    for B, want in cases:
+        A, U, Z, info = oracle.hsvd2(np.array(B), [-1, 1], th1=1.0)
+        assert info == want
+        A, U, Z, info = oracle.hsvd2(np.array(B), [-1, 1], th1=0.75)
+        assert info == want
+    # exactly equal columns: most seeded blocks fail with -10 (the rest pass by rounding)
+    rng = np.random.default_rng(7)
+    fails = 0
+    for _ in range(400):
+        B = rng.standard_normal((2, 2))
+        B[:, 1] = B[:, 0]
+        A, U, Z, info = oracle.hsvd2(B, [-1, 1], th1=1.0)
+        assert info in (-10, 7)
+        fails += info == -10
+    assert fails > 200
