@@ -369,8 +369,10 @@ __device__ __forceinline__ void scan_chunk_kw(int kw, const double *const *xs, c
 // parameters of the pairs that need the column scan, compacted into shared memory that
 // the row buffer reuses once every thread holds its own pairs' parameters; the other
 // weights straight to W), then the tile's 64 columns stream through a three-stage
-// buffer in row chunks and every thread runs its pairs' fma chains.  A warp whose pairs
-// have none of their rows p, q in a chunk runs that chunk without the per-row skip test.
+// buffer in row chunks and every thread runs its pairs' fma chains.  Only the 32-row
+// sub-blocks of a chunk that hold a row p or q of some pair of the warp run the per-row
+// skip test, and a warp whose pairs all have the same orientation loads the column its
+// thread's pairs share once per row pair.
 __global__ void __launch_bounds__(SCAN_THREADS, 2)
 k_hyp_pm(const State *st, const double *__restrict__ A, const int *__restrict__ plus, const int *__restrict__ minus,
          int n_plus, int n_minus, int n, double *__restrict__ Wm)
