@@ -491,7 +491,7 @@ def run_ours(args, wl):
     flops = nh * (n - 2) * (14 if not cplx else 36)  # NH (N - 2) rows x the per-row flops of the off-norm scan
     achieved = flops / (w_ms * 1e-3) / 1e12
     peak = jk.lib().jk_fp64_peak()
-    traffic = _recorded_traffic(args.workload)
+    traffic, traffic_warm = _recorded_traffic(args.workload)
 
     if ws > 1:
         dist.barrier()
@@ -523,6 +523,9 @@ def run_ours(args, wl):
         "gpu_launches": launches,
         "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                      "frac": achieved / peak if peak > 0 else None, "traffic": traffic,
+                     "traffic_warm_l2": traffic_warm,
+                     "traffic_note": "traffic: ncu DRAM bytes of one k_hyp_pm launch with L2 flushed before it; "
+                                     "traffic_warm_l2: the same launch after the trig-weight kernel, as in a build",
                      "kernel": "pair weights (k_weights_trig + k_hyp_pm), timed alone on the input Y",
                      "algorithmic_flop_per_launch": flops, "launch_ms": w_ms,
                      "peak_note": "FP64 FMA throughput measured live by jk_fp64_peak; the weight scan's op mix "
@@ -566,11 +569,16 @@ def _sigma_err(sig, ref, J):
 
 
 def _recorded_traffic(workload):
+    """DRAM bytes of one launch of the weight kernel from the committed ncu captures: (cold-cache
+    capture, capture with the cache as a build leaves it), None where there is none."""
     try:
         rec = json.load(open(os.path.join(ROOT, "profiles", "traffic.json"))).get(workload)
-        return float(rec["bytes_per_launch"]) if rec else None
     except Exception:
-        return None
+        return None, None
+    if not rec:
+        return None, None
+    warm = rec.get("bytes_per_launch_warm_l2")
+    return float(rec["bytes_per_launch"]), (float(warm) if warm is not None else None)
 
 
 def main():

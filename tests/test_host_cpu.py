@@ -31,3 +31,15 @@ def test_graded_generator_scales():
     norms = np.linalg.norm(Y, axis=0)
     assert norms.max() / norms.min() > 1e3
     assert int(np.sum(J == 1)) == 32 and int(np.sum(J == -1)) == 32
+
+
+def test_bench_recorded_traffic():
+    """bench.py's roofline takes the weight kernel's DRAM bytes per launch from the committed ncu
+    captures: the cold-cache figure and the one with the cache as a build leaves it."""
+    import os
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    import bench
+    cold, warm = bench._recorded_traffic("djk_n2048_graded")
+    assert cold is not None and warm is not None and 0 < warm < cold
+    assert bench._recorded_traffic("no_such_workload") == (None, None)
