@@ -77,7 +77,12 @@ int jk_zstep_loop(int n, double *U, int ldu, double *A, int lda, double *Z, int 
 
 /* The same loops on device buffers (leading dimension n), enqueued on `stream`
  * (a cudaStream_t, NULL = the default stream); J is a host array.  Synchronises the
- * stream before returning INFO. */
+ * stream before returning INFO.  Device buffers must be aligned as cudaMalloc returns them:
+ * 8 bytes for real data, 16 for complex data and for A of a scored real solve
+ * (jk_dstep_loop_dev_scored).  A NULL or misaligned U, A, Z or SIGMA returns -2, -4, -6
+ * or -9, its position in DSTEP_LOOP's argument list, before anything runs on the device;
+ * the same check makes jk_solver_begin / resume / finish return -2, jk_handle_weights and
+ * the jk_batch_run / jk_batch_tune buffers -1. */
 int jk_dstep_loop_dev(int n, double *dU, double *dA, double *dZ, const int *J, double *dsigma,
                       int n_2, int id_ncp, int id_tru, const jk_opts *opts, jk_trace *trace, void *stream);
 int jk_zstep_loop_dev(int n, double *dU, double *dA, double *dZ, const int *J, double *dsigma,

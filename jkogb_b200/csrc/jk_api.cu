@@ -1,6 +1,7 @@
 // jk_api.cu -- the C ABI of libjkogb_b200.so (include/jkogb.h): device workspaces,
 // the step-loop driver (CUDA graphs of whole steps, a device-side stop flag read
 // back between graph launches) and the kernel-level entry points.
+#include <cstdint>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -356,6 +357,22 @@ int run_loop(int cplx, int n, void *dU, void *dA, void *dZ, const int *J, double
   return solver_finish(&v, dsigma, exact_steps);
 }
 
+// a device buffer argument: not NULL and aligned as the kernels read it (8 bytes for real
+// data; 16 for complex data, and for A of a scored real solve, whose Gram kernel copies 16
+// bytes at a time)
+bool dev_ok(const void *p, size_t align) { return p && !((uintptr_t)p & (uintptr_t)(align - 1)); }
+
+// the device matrices of a loop entry, reported by their position in DSTEP_LOOP's argument
+// list (src/D/dstep.F90:472-482: U 2, A 4, Z 6; SIGMA is 9), as its INFO reports bad arguments
+int check_dev(int cplx, int scored, const void *dU, const void *dA, const void *dZ)
+{
+  const size_t m = cplx ? 16 : 8;
+  if (!dev_ok(dU, m)) return -2;
+  if (!dev_ok(dA, (cplx || scored) ? 16 : 8)) return -4;
+  if (!dev_ok(dZ, m)) return -6;
+  return 0;
+}
+
 int pick_device(const jk_opts *opts)
 {
   int cnt = 0;
@@ -416,7 +433,9 @@ int jk_zstep_loop(int n, double *U, int ldu, double *A, int lda, double *Z, int 
 int jk_dstep_loop_dev(int n, double *dU, double *dA, double *dZ, const int *J, double *dsigma, int n_2, int id_ncp, int id_tru,
                       const jk_opts *opts, jk_trace *trace, void *stream)
 {
-  const int rc = check_args(n, n, n, n, J, n_2, id_ncp, id_tru, 0);
+  int rc = check_args(n, n, n, n, J, n_2, id_ncp, id_tru, 0);
+  if (!rc) rc = check_dev(0, 0, dU, dA, dZ);
+  if (!rc && !dev_ok(dsigma, 8)) rc = -9;
   if (rc) return rc;
   return run_loop(0, n, dU, dA, dZ, J, dsigma, n_2, id_ncp, id_tru, opts, trace, (cudaStream_t)stream);
 }
@@ -424,7 +443,9 @@ int jk_dstep_loop_dev(int n, double *dU, double *dA, double *dZ, const int *J, d
 int jk_zstep_loop_dev(int n, double *dU, double *dA, double *dZ, const int *J, double *dsigma, int n_2, int id_ncp, int id_tru,
                       const jk_opts *opts, jk_trace *trace, void *stream)
 {
-  const int rc = check_args(n, n, n, n, J, n_2, id_ncp, id_tru, 1);
+  int rc = check_args(n, n, n, n, J, n_2, id_ncp, id_tru, 1);
+  if (!rc) rc = check_dev(1, 0, dU, dA, dZ);
+  if (!rc && !dev_ok(dsigma, 8)) rc = -9;
   if (rc) return rc;
   return run_loop(1, n, dU, dA, dZ, J, dsigma, n_2, id_ncp, id_tru, opts, trace, (cudaStream_t)stream);
 }
@@ -449,14 +470,14 @@ void jk_solver_destroy(jk_solver *v) { delete v; }
 int jk_solver_begin(jk_solver *v, double *dU, double *dA, double *dZ, void *stream)
 {
   if (!v) return -1;
-  if (!dU || !dA || !dZ) return -2;
+  if (check_dev(v->cplx, 0, dU, dA, dZ)) return -2;
   return solver_start(v, dU, dA, dZ, nullptr, 0, (cudaStream_t)stream);
 }
 
 int jk_solver_resume(jk_solver *v, double *dU, double *dA, double *dZ, const double *dsigma, long long steps, void *stream)
 {
   if (!v) return -1;
-  if (!dU || !dA || !dZ || !dsigma) return -2;
+  if (!dev_ok(dsigma, 8) || check_dev(v->cplx, 0, dU, dA, dZ)) return -2;
   // a complex loop's end keeps only the real parts of the diagonal in SIGMA
   if (v->cplx) return JK_ERR_STATE;
   return solver_start(v, dU, dA, dZ, dsigma, steps, (cudaStream_t)stream);
@@ -474,7 +495,7 @@ long long jk_solver_steps(const jk_solver *v) { return v ? v->steps : -1; }
 int jk_solver_finish(jk_solver *v, double *dsigma)
 {
   if (!v) return -1;
-  if (!dsigma) return -2;
+  if (!dev_ok(dsigma, 8)) return -2;
   return solver_finish(v, dsigma, nullptr);
 }
 
@@ -581,7 +602,7 @@ void jk_handle_destroy(jk_handle *h) { delete h; }
 
 int jk_handle_weights(jk_handle *h, const double *dA, double *dW, void *stream)
 {
-  if (!h || !dA) return -1;
+  if (!h || !dev_ok(dA, h->w.cplx ? 16 : 8)) return -1;
   cudaStream_t s = (cudaStream_t)stream;
   CK(launch_weights(h->w, dA, s));
   if (dW) CK(cudaMemcpyAsync(dW, h->w.Wm, (size_t)h->w.n * h->w.n * sizeof(double), cudaMemcpyDeviceToDevice, s));
@@ -700,7 +721,7 @@ void jk_batch_destroy(jk_batch *b) { delete b; }
 
 int jk_batch_run(jk_batch *b, double *dA, double *dU, double *dZ, double *dsigma, int *dinfo, void *stream)
 {
-  if (!b || !dA || !dU || !dZ || !dsigma || !dinfo) return -1;
+  if (!b || !dev_ok(dA, 8) || !dev_ok(dU, 8) || !dev_ok(dZ, 8) || !dev_ok(dsigma, 8) || !dev_ok(dinfo, 4)) return -1;
   cudaStream_t s = (cudaStream_t)stream;
   const void *key[6] = { dA, dU, dZ, dsigma, dinfo, stream };
   bool same = (b->exec != nullptr) && (b->key_variant == b->variant) && (b->key_scored == b->scored);
@@ -746,7 +767,7 @@ int jk_batch_set_scorer(jk_batch *b, const jk_scorer *sc)
 
 int jk_batch_tune(jk_batch *b, const double *dA, double *dU, double *dZ, double *dsigma, int *dinfo, void *stream)
 {
-  if (!b || !dA || !dU || !dZ || !dsigma || !dinfo) return -1;
+  if (!b || !dev_ok(dA, 8) || !dev_ok(dU, 8) || !dev_ok(dZ, 8) || !dev_ok(dsigma, 8) || !dev_ok(dinfo, 4)) return -1;
   cudaStream_t s = (cudaStream_t)stream;
   Guard g;
   double *scratch = nullptr;
@@ -863,7 +884,9 @@ int jk_dstep_loop_dev_scored(int n, double *dU, double *dA, double *dZ, const in
                              const jk_scorer *sc, const jk_opts *opts, jk_trace *trace, int *exact_steps, void *stream)
 {
   if (!sc) return -9;
-  const int rc = check_args(n, n, n, n, J, n_2, 0, 0, 0);
+  int rc = check_args(n, n, n, n, J, n_2, 0, 0, 0);
+  if (!rc) rc = check_dev(0, 1, dU, dA, dZ);
+  if (!rc && !dev_ok(dsigma, 8)) rc = -9;
   if (rc) return rc;
   return run_loop(0, n, dU, dA, dZ, J, dsigma, n_2, 0, 0, opts, trace, (cudaStream_t)stream, sc, exact_steps);
 }
@@ -872,7 +895,9 @@ int jk_zstep_loop_dev_scored(int n, double *dU, double *dA, double *dZ, const in
                              const jk_scorer *sc, const jk_opts *opts, jk_trace *trace, int *exact_steps, void *stream)
 {
   if (!sc) return -9;
-  const int rc = check_args(n, n, n, n, J, n_2, 0, 0, 1);
+  int rc = check_args(n, n, n, n, J, n_2, 0, 0, 1);
+  if (!rc) rc = check_dev(1, 1, dU, dA, dZ);
+  if (!rc && !dev_ok(dsigma, 8)) rc = -9;
   if (rc) return rc;
   return run_loop(1, n, dU, dA, dZ, J, dsigma, n_2, 0, 0, opts, trace, (cudaStream_t)stream, sc, exact_steps);
 }
@@ -880,7 +905,7 @@ int jk_zstep_loop_dev_scored(int n, double *dU, double *dA, double *dZ, const in
 static long long features(int cplx, int n, const double *dA, const int *J, int step, float *dX, double *dWg,
                           void *stream)
 {
-  if (n < 3 || !dA || !J || !dX) return -1;
+  if (n < 3 || !dev_ok(dA, 16) || !J || !dX) return -1;
   std::vector<int> plus, minus;
   for (int i = 0; i < n; ++i) {
     if (J[i] == 1) plus.push_back(i);

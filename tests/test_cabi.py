@@ -102,3 +102,31 @@ def test_ncp3_order_limit_without_gpu():
     d = lambda a: a.ctypes.data  # noqa: E731
     Jp = J.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
     assert L.jk_dstep_loop(n, d(A), n, d(A), n, d(A), n, Jp, d(A), 0, 3, 0, ctypes.byref(o), None) == -32
+
+
+def test_device_buffer_checks_without_gpu():
+    """NULL or misaligned device buffers are rejected with DSTEP_LOOP's argument positions
+    (U -2, A -4, Z -6, SIGMA -9) before anything reaches a device.  Every call below has at
+    least one such buffer, so none of them runs a kernel on the fake addresses."""
+    import numpy as np
+    import jkogb_b200 as jk
+    L = jk.lib()
+    n = 4
+    J = np.array([1, 1, -1, -1], np.int32)
+    Jp = J.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+    o = jk.Opts()
+    ok16, ok8, bad8, bad16 = 0x100000, 0x200000, 0x300004, 0x400008  # bad16: 8- but not 16-byte aligned
+    V = ctypes.c_void_p
+    def d(*a):  # noqa: E306
+        return L.jk_dstep_loop_dev(n, V(a[0]), V(a[1]), V(a[2]), Jp, V(a[3]), 0, 0, 0, ctypes.byref(o), None, None)
+    def z(*a):  # noqa: E306
+        return L.jk_zstep_loop_dev(n, V(a[0]), V(a[1]), V(a[2]), Jp, V(a[3]), 0, 0, 0, ctypes.byref(o), None, None)
+    assert d(None, ok8, ok8, ok8) == -2
+    assert d(ok8, bad8, ok8, ok8) == -4
+    assert d(ok8, ok8, None, ok8) == -6
+    assert d(ok8, ok8, ok8, None) == -9
+    assert d(ok8, ok8, ok8, bad8) == -9
+    assert z(bad16, ok16, ok16, ok8) == -2
+    assert z(ok16, bad16, ok16, ok8) == -4
+    assert z(ok16, ok16, bad16, ok8) == -6
+    assert z(ok16, ok16, ok16, bad8) == -9
